@@ -1,0 +1,344 @@
+#!/usr/bin/env python
+"""Benchmark of the plain wavefront path tracer at scale (Mrays/s at 1080p / 1.31M triangles).
+
+Workload (one GPU): seeded displaced-icosphere field, 64 instances x 20,480 triangles (1.31M f32
+triangles), 16-layer 1024^2 value-noise textures, 1920x1080, Medium shader, depth 12, no guiding,
+ReSTIR off.  One step = one lam_render of 16 samples per pixel; 16 steps make the 256-spp image.
+
+  python bench.py [--gpus N --steps K --warmup W]            this implementation (CUDA, sm_100a)
+  python bench.py --impl reference [...]                     the reference path on the host cores
+                                                             (CPU restatement of its shaders)
+Multi-GPU (torchrun, one rank per GPU): every rank renders its own samples of the full frame with
+a distinct seed (sample sharding, weak scaling); the images are summed with one NCCL all-reduce at
+the end of the timed region.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mrays/s at 1080p/1.3M tris"
+SEG_BYTES_EXTEND = 48   # ray (o, d, tmax) 28 B read + hit 20 B write per segment
+SEG_BYTES_TOTAL = 280   # extend 48 + shade 232 (compulsory wavefront traffic per segment)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=16)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--spp", type=int, default=16, help="samples per pixel per step")
+    p.add_argument("--depth", type=int, default=12)
+    p.add_argument("--width", type=int, default=1920)
+    p.add_argument("--height", type=int, default=1080)
+    p.add_argument("--instances", type=int, default=64)
+    p.add_argument("--subdiv", type=int, default=5)
+    p.add_argument("--tex", type=int, default=1024)
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--out", default=None, help="also write the JSON line to this file")
+    return p.parse_args()
+
+
+def workload_config(a):
+    return {
+        "workload": f"icosphere field {a.instances}x{20 * 4 ** a.subdiv} tris, {a.width}x{a.height}, "
+                    f"{a.spp} spp/step, depth {a.depth}, Medium, plain (no guiding, ReSTIR off)",
+        "triangles": a.instances * 20 * 4 ** a.subdiv,
+        "resolution": [a.width, a.height],
+        "spp_per_step": a.spp,
+        "max_depth": a.depth,
+        "textures": f"3 x 16 layers {a.tex}^2 RGBA8 value noise",
+        "cache": "inputs larger than L2: path state + textures + triangles exceed 126 MB",
+    }
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, index):
+        self.index, self.samples, self.stop_flag = index, [], threading.Event()
+        self.t = threading.Thread(target=self.run, daemon=True)
+
+    def run(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        while not self.stop_flag.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                vals = [v.strip() for v in out.stdout.strip().split(",")]
+                if len(vals) == 6:
+                    self.samples.append(vals)
+            except Exception:
+                pass
+            self.stop_flag.wait(0.2)
+
+    def __enter__(self):
+        self.t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self.stop_flag.set()
+        self.t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = sorted(float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit())
+        mx = max((float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[2 + i]})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def build_scene(a):
+    from lambent_b200 import scenes
+    return scenes.icosphere_field(a.width, a.height, instances=a.instances, subdiv=a.subdiv, tex_size=a.tex)
+
+
+def cpu_reference(a, scene, seconds):
+    """The reference path on the host cores: the CPU restatement of its shaders, a crop of the
+    same frame (full-frame rays and seeds) sized to about `seconds` of work."""
+    from oracle import oracle_py as O
+    from lambent_b200 import _abi
+    cores = os.cpu_count() or 1
+    osc = O.OracleScene(scene)
+    x0, y0 = a.width // 2 - 32, a.height // 2 - 32
+    w = h = 64
+    spp = 2
+    t0 = time.perf_counter()
+    r = osc.render(scene.camera, a.width, a.height, samples=spp, max_depth=a.depth, restir=_abi.RESTIR_DISABLED,
+                   crop=(x0, y0, w, h), threads=cores)
+    dt = time.perf_counter() - t0
+    # grow the crop towards the time budget (square, centred), keep at least one calibration run
+    scale = max(1.0, min(64.0, seconds / max(dt, 1e-3)))
+    side = int(min(min(a.width, a.height), 64 * scale ** 0.5)) // 32 * 32
+    if side > 64:
+        x0, y0 = a.width // 2 - side // 2, a.height // 2 - side // 2
+        t0 = time.perf_counter()
+        r = osc.render(scene.camera, a.width, a.height, samples=spp, max_depth=a.depth, restir=_abi.RESTIR_DISABLED,
+                       crop=(x0, y0, side, side), threads=cores)
+        dt = time.perf_counter() - t0
+        w = h = side
+    mrays = r["segments"] / dt / 1e6
+    return {"value": round(mrays, 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
+            "sample": f"centre crop {w}x{h} of the {a.width}x{a.height} frame, {spp} spp, depth {a.depth}, "
+                      f"{r['segments']} segments in {dt:.2f} s",
+            "samples_per_s": round(r["samples"] / dt, 1)}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    scene = build_scene(a)
+    base = cpu_reference(a, scene, a.cpu_seconds)
+    steps_ms = []
+    # each step is a bounded sample of the workload; value = Mrays/s over the steps
+    from oracle import oracle_py as O
+    from lambent_b200 import _abi
+    osc = O.OracleScene(scene)
+    cores = os.cpu_count() or 1
+    side = 64
+    segs = 0
+    tot = 0.0
+    for k in range(a.warmup + a.steps):
+        x0, y0 = a.width // 2 - side // 2, a.height // 2 - side // 2
+        t0 = time.perf_counter()
+        r = osc.render(scene.camera, a.width, a.height, samples=2, max_depth=a.depth, restir=_abi.RESTIR_DISABLED,
+                       crop=(x0, y0, side, side), threads=cores, seed_offset=k)
+        dt = time.perf_counter() - t0
+        if k >= a.warmup:
+            segs += r["segments"]
+            tot += dt
+            steps_ms.append(dt * 1e3)
+    v = segs / tot / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "Mrays/s", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(sum(steps_ms) / len(steps_ms), 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(a),
+            "cpu_baseline": {"value": round(v, 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
+                             "sample": f"per step: centre crop {side}x{side}, 2 spp, depth {a.depth} "
+                                       "(the reference's wgpu shaders need a graphics stack, unavailable on this box; "
+                                       "this is the CPU restatement of those shaders)"},
+            "e2e": {"value": round(v, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "calibration": base}
+    emit(line, a)
+
+
+def emit(line, a):
+    s = json.dumps(line)
+    print(s, flush=True)
+    if a.out:
+        with open(a.out, "w") as f:
+            f.write(s + "\n")
+
+
+def run_ours(a):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import lambent_b200 as lb
+    from lambent_b200 import _abi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+
+    scene = build_scene(a)
+    gscene = lb.GpuScene(scene)
+    st = gscene.stats()
+    tracer = lb.RayTracer(lb.path_tracing.Medium)
+    opts = lb.PathTracerOpts(samples=a.spp, restir_temporal=lb.RestirTemporalMode.Disabled, max_depth=a.depth,
+                             guide_mode=lb.GuideMode.NONE)
+    pipe = tracer.create_pipeline(*scene.layout_counts(), opts)
+    bufs = lb.DataBuffers(a.width, a.height, 1, 0)
+    H, W = a.height, a.width
+    color = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
+    normal = torch.zeros_like(color)
+    albedo = torch.zeros_like(color)
+    tg = lb.targets_from(color, normal, albedo)
+    seed0 = rank * 1_000_003
+
+    for k in range(a.warmup):
+        pipe.render(gscene, bufs, scene.camera, tg, seed0 + k, stream)
+    torch.cuda.synchronize()
+    pipe.set_profiling(True)
+    pipe.profile_reset()
+    accum = torch.zeros_like(color)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        start.record(stream)
+        for k in range(a.steps):
+            pipe.render(gscene, bufs, scene.camera, tg, seed0 + a.warmup + k, stream)
+            accum.add_(color)
+        if world > 1:
+            dist.all_reduce(accum)
+        end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = start.elapsed_time(end)
+    prof = pipe.profile()
+    pipe.set_profiling(False)
+    launches = pipe.stats().kernel_launches * a.steps
+    segs = prof.ray_segments
+    t = torch.tensor([ms, float(segs), float(prof.extend_ms), float(prof.shade_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = t.clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        ms_max, segs_total = tmax[0].item(), tsum[1].item()
+    else:
+        ms_max, segs_total = ms, float(segs)
+    value = segs_total / (ms_max / 1e3) / 1e6
+
+    # e2e through the public API with host buffers: camera H2D + render + colour D2H per step
+    pinned_cam = torch.empty(32, dtype=torch.float32).pin_memory()
+    pinned_cam.copy_(torch.tensor(list(scene.camera.c.projection_inverse) + list(scene.camera.c.view_inverse)))
+    cam_dev = torch.empty(32, dtype=torch.float32, device=dev)
+    host_img = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    pipe.profile_reset()
+    pipe.set_profiling(True)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(a.steps):
+        cam_dev.copy_(pinned_cam, non_blocking=True)
+        pipe.render(gscene, bufs, scene.camera, tg, seed0 + 7777 + k, stream)
+        host_img.copy_(color, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    e2e_prof = pipe.profile()
+    pipe.set_profiling(False)
+    tt = torch.tensor([e2e_ms, float(e2e_prof.ray_segments)], dtype=torch.float64, device=dev)
+    if world > 1:
+        m = tt.clone()
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        s_ = tt.clone()
+        dist.all_reduce(s_, op=dist.ReduceOp.SUM)
+        e2e_ms_max, e2e_segs = m[0].item(), s_[1].item()
+    else:
+        e2e_ms_max, e2e_segs = e2e_ms, float(e2e_prof.ray_segments)
+    e2e_value = e2e_segs / (e2e_ms_max / 1e3) / 1e6
+
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        ext_s = prof.extend_ms / 1e3
+        achieved = segs * SEG_BYTES_EXTEND / ext_s / 1e9 if ext_s > 0 else 0.0
+        shade_s = prof.shade_ms / 1e3
+        shade_gbs = segs * (SEG_BYTES_TOTAL - SEG_BYTES_EXTEND) / shade_s / 1e9 if shade_s > 0 else 0.0
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(a),
+            "samples_per_s": round(W * H * a.spp * a.steps * world / (ms_max / 1e3), 1),
+            "roofline": {"bound": "hbm", "kernel": "extend_kernel (BVH8 traversal)",
+                         "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 5), "peak_kind": f"{peak_kind} hbm_gbs",
+                         "bytes_per_segment": SEG_BYTES_EXTEND, "traffic": None,
+                         "extend_ms": round(prof.extend_ms, 3), "shade_ms": round(prof.shade_ms, 3),
+                         "generate_ms": round(prof.generate_ms, 3), "accumulate_ms": round(prof.accumulate_ms, 3),
+                         "shade_gbs": round(shade_gbs, 2)},
+            "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 128,
+                    "d2h_bytes_per_step": H * W * 16},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+            "scene": {"triangles": st.triangle_count, "blas_nodes": st.blas_node_count,
+                      "tlas_nodes": st.tlas_node_count, "device_bytes": st.device_bytes,
+                      "build_s": round(st.build_seconds, 3)},
+        }
+        if not a.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_reference(a, scene, a.cpu_seconds)
+        emit(line, a)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,251 @@
+// guide.cuh - the reference's vMF Markov-chain guiding on the device
+// (src/path_tracing/general.wesl:147-500 and 984-1047).
+//
+// World grid: WorldMarcovChainState records (56 bytes, src/bindings.wesl:33-40) as 14 u32 words,
+// updated with the same protocol as the shader: CAS-claim of the secondary hash, try-lock for
+// the radiance sum (a locked cell is skipped, never waited on), relaxed stores of the chain.
+#pragma once
+#include "../../include/lambent.h"
+#include "device_math.cuh"
+
+namespace lam {
+
+struct MC {
+    v3 light;
+    float mean_cosine, weight_sum;
+    uint32_t num_samples;
+    float score;
+};
+
+LAM_DEV MC mc_zero() {
+    MC s;
+    s.light = splat(0.0f);
+    s.mean_cosine = 0.0f;
+    s.weight_sum = 0.0f;
+    s.num_samples = 0u;
+    s.score = 0.0f;
+    return s;
+}
+
+LAM_DEV MC mc_from(const lam_markov_chain& c) {
+    MC s;
+    s.light = mk(c.light_source[0], c.light_source[1], c.light_source[2]);
+    s.mean_cosine = c.mean_cosine;
+    s.weight_sum = c.weight_sum;
+    s.num_samples = c.num_samples;
+    s.score = c.score;
+    return s;
+}
+
+LAM_DEV MC mc_load(const lam_markov_chain* p) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+    float4 a = q[0], b = q[1];
+    MC s;
+    s.light = mk(a.x, a.y, a.z);
+    s.mean_cosine = a.w;
+    s.weight_sum = b.x;
+    s.num_samples = __float_as_uint(b.y);
+    s.score = b.z;
+    return s;
+}
+
+LAM_DEV void mc_store(lam_markov_chain* p, const MC& s) {
+    float4* q = reinterpret_cast<float4*>(p);
+    q[0] = make_float4(s.light.x, s.light.y, s.light.z, s.mean_cosine);
+    q[1] = make_float4(s.weight_sum, __uint_as_float(s.num_samples), s.score, 0.0f);
+}
+
+constexpr int W_SEC = 0, W_NUM = 1, W_LUM = 2, W_LOCK = 5, W_CL = 6, W_CMEAN = 9, W_CWS = 10, W_CNUM = 11,
+              W_CSCORE = 12, W_TIMEOUT = 13, W_STRIDE = 14;
+constexpr uint32_t CACHE_TIMEOUT = 30u;
+constexpr uint32_t MAX_NUM_SAMPLES = 0x0FFFFFFFu;
+constexpr int NUM_RESAMPLES = 21;
+
+LAM_DEV uint32_t vload(const uint32_t* p) { return *(const volatile uint32_t*)p; }
+LAM_DEV void vstore(uint32_t* p, uint32_t v) { *(volatile uint32_t*)p = v; }
+
+struct Grid {
+    uint32_t* world;
+    const uint32_t* old_world;
+    uint64_t len;
+    v3 camera_loc;
+};
+
+struct IVec { int32_t x, y, z; };
+
+LAM_DEV IVec grid_loc(const Grid& g, v3 pos) {
+    v3 diff = pos - g.camera_loc;
+    float len = fmaxf(fabsf(diff.x), fmaxf(fabsf(diff.y), fabsf(diff.z)));
+    uint32_t shifts = f2u(log2f(fmaxf(len / 1.0f, 1.0f)));
+    uint32_t mask = 0xFFFFFFFFu << min(shifts, 30u);
+    IVec r{f2i(pos.x / 0.1f), f2i(pos.y / 0.1f), f2i(pos.z / 0.1f)};
+    r.x &= (int32_t)mask;
+    r.y &= (int32_t)mask;
+    r.z &= (int32_t)mask;
+    return r;
+}
+
+LAM_DEV uint32_t primary_hash(IVec l, v3 normal, v3 incoming) {
+    uint32_t n = normalised_to_u32(normal) & 0xFF00FF00u;
+    uint32_t ih = (uint32_t)(incoming.x > 0.0f) | ((uint32_t)(incoming.y > 0.0f) << 1) | ((uint32_t)(incoming.z > 0.0f) << 2);
+    uint32_t inc = rand_u32(ih);
+    return ((((uint32_t)l.x * 1u) ^ ((uint32_t)l.y * 687603047u)) ^ ((uint32_t)l.z * 571899763u)) ^ (n * 894271171u) ^
+           (inc * 840057787u);
+}
+
+LAM_DEV uint32_t secondary_hash(IVec l, v3 normal) {
+    uint32_t n = normalised_to_u32(normal) & 0xFF00FF00u;
+    uint32_t h = (((uint32_t)l.x * 1699644091u) ^ ((uint32_t)l.y * 550105817u)) ^ ((uint32_t)l.z * 956114303u);
+    return (rand_u32(h) ^ (n * 155096983u)) | 1u;
+}
+
+LAM_DEV MC read_chain(const uint32_t* e) {
+    MC s;
+    s.light = mk(__uint_as_float(vload(e + W_CL)), __uint_as_float(vload(e + W_CL + 1)), __uint_as_float(vload(e + W_CL + 2)));
+    s.mean_cosine = __uint_as_float(vload(e + W_CMEAN));
+    s.weight_sum = __uint_as_float(vload(e + W_CWS));
+    s.num_samples = vload(e + W_CNUM);
+    s.score = __uint_as_float(vload(e + W_CSCORE));
+    return s;
+}
+
+LAM_DEV MC grid_load(const Grid& g, v3 pos, v3 normal, v3 incoming, bool force_old) {
+    IVec l = grid_loc(g, pos);
+    uint64_t idx = primary_hash(l, normal, incoming) % g.len;
+    uint32_t* e = g.world + idx * W_STRIDE;
+    uint32_t sec = secondary_hash(l, normal);
+    MC s = read_chain(e);
+    if (vload(e + W_SEC) != sec || force_old) {
+        const uint32_t* o = g.old_world ? g.old_world + idx * W_STRIDE : nullptr;
+        if (o && vload(o + W_SEC) == sec) s = read_chain(o);
+        else s = mc_zero();
+    } else {
+        vstore(e + W_TIMEOUT, CACHE_TIMEOUT);
+    }
+    s.light = strip_nan3(s.light);
+    s.mean_cosine = strip_nan(s.mean_cosine);
+    s.weight_sum = strip_nan(s.weight_sum);
+    s.score = strip_nan(s.score);
+    return s;
+}
+
+LAM_DEV void grid_store(const Grid& g, v3 pos, v3 normal, v3 incoming, const MC& st) {
+    IVec l = grid_loc(g, pos);
+    uint64_t idx = primary_hash(l, normal, incoming) % g.len;
+    uint32_t* e = g.world + idx * W_STRIDE;
+    uint32_t sec = secondary_hash(l, normal);
+    if (vload(e + W_SEC) != sec) {
+        if (atomicCAS(e + W_SEC, 0u, sec) != 0u) return;
+    }
+    vstore(e + W_CL, __float_as_uint(st.light.x));
+    vstore(e + W_CL + 1, __float_as_uint(st.light.y));
+    vstore(e + W_CL + 2, __float_as_uint(st.light.z));
+    vstore(e + W_CMEAN, __float_as_uint(st.mean_cosine));
+    vstore(e + W_CWS, __float_as_uint(st.weight_sum));
+    vstore(e + W_CNUM, st.num_samples);
+    vstore(e + W_CSCORE, __float_as_uint(st.score));
+    vstore(e + W_TIMEOUT, CACHE_TIMEOUT);
+}
+
+LAM_DEV v3 grid_radiance(const Grid& g, v3 pos, v3 normal, v3 incoming) {
+    IVec l = grid_loc(g, pos);
+    uint64_t idx = primary_hash(l, normal, incoming) % g.len;
+    uint32_t* e = g.world + idx * W_STRIDE;
+    uint32_t num = vload(e + W_NUM);
+    v3 rad = mk(__uint_as_float(vload(e + W_LUM)), __uint_as_float(vload(e + W_LUM + 1)), __uint_as_float(vload(e + W_LUM + 2)));
+    uint32_t sec = secondary_hash(l, normal);
+    if (vload(e + W_SEC) != sec) {
+        const uint32_t* o = g.old_world ? g.old_world + idx * W_STRIDE : nullptr;
+        if (o && vload(o + W_SEC) == sec) {
+            num = vload(o + W_NUM);
+            rad = mk(__uint_as_float(vload(o + W_LUM)), __uint_as_float(vload(o + W_LUM + 1)), __uint_as_float(vload(o + W_LUM + 2)));
+        } else {
+            return splat(0.0f);
+        }
+    } else {
+        vstore(e + W_TIMEOUT, CACHE_TIMEOUT);
+    }
+    if (num == 0u) return splat(0.0f);
+    return clamp3(rad / __uint2float_rn(num), 0.0f, 1000.0f);
+}
+
+LAM_DEV void grid_add_radiance(const Grid& g, v3 pos, v3 normal, v3 incoming, v3 radiance) {
+    IVec l = grid_loc(g, pos);
+    uint64_t idx = primary_hash(l, normal, incoming) % g.len;
+    uint32_t* e = g.world + idx * W_STRIDE;
+    uint32_t sec = secondary_hash(l, normal);
+    v3 c = clamp3(radiance, 0.0f, 100.0f);
+    if (vload(e + W_SEC) != sec) {
+        if (atomicCAS(e + W_SEC, 0u, sec) != 0u) return;
+    }
+    // try-lock: a locked cell is skipped (the shader must make forward progress)
+    if (atomicExch(e + W_LOCK, 1u) == 1u) return;
+    __threadfence();
+    uint32_t num = vload(e + W_NUM);
+    if (num >= MAX_NUM_SAMPLES) {
+        __threadfence();
+        atomicExch(e + W_LOCK, 0u);
+        vstore(e + W_TIMEOUT, CACHE_TIMEOUT);
+        return;
+    }
+    atomicAdd(e + W_NUM, 1u);
+    float cc[3] = {c.x, c.y, c.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float r = strip_nan(cc[k] + __uint_as_float(vload(e + W_LUM + k)));
+        vstore(e + W_LUM + k, __float_as_uint(fmaxf(r, 0.0f)));
+    }
+    __threadfence();
+    atomicExch(e + W_LOCK, 0u);
+    vstore(e + W_TIMEOUT, CACHE_TIMEOUT);
+}
+
+LAM_DEV v3 light_dir(const MC& s, v3 cur) { return safe_div3(s.light, s.weight_sum) - cur; }
+
+LAM_DEV float get_kappa(const MC& s) {
+    const float Np = 0.2f, rp = 0.99f;
+    float N2 = __uint2float_rn(s.num_samples * s.num_samples);
+    float r = ((N2 * (s.mean_cosine / s.weight_sum)) + (Np * rp)) / (N2 + Np);
+    return clampf(((3.0f * r) - ((r * r) * r)) / (1.0f - (r * r)), 0.001f, 8.50705867e37f);
+}
+
+LAM_DEV float exp_minus_one(float x) {
+    float u = expf(x);
+    if (u == 1.0f) return x;
+    float y = u - 1.0f;
+    if (fabsf(x) < 1.0f) return (x * y) / logf(u);
+    return y;
+}
+
+LAM_DEV float x_div_exp_minus_one(float x) {
+    float u = expf(x);
+    if (u == 1.0f) return 1.0f;
+    float y = u - 1.0f;
+    if (fabsf(x) < 1.0f) return logf(u) / y;
+    return x / y;
+}
+
+LAM_DEV float vmf_pdf(v3 mean, float kappa, v3 dir) {
+    float fraction = x_div_exp_minus_one(-2.0f * kappa) / (4.0f * PI_F);
+    return fmaxf(fraction * expf(kappa * (dot(dir, mean) - 1.0f)), 0.0f);
+}
+
+// update_marcov_state, general.wesl:464-492 (sum_mc: the candidate weight sum of the last resample)
+LAM_DEV MC update_chain(v3 x1, v3 x2, float p_hat, uint32_t seed, bool not_vmf, MC state, float confidence,
+                        float sum_mc) {
+    if (not_vmf) state = mc_zero();
+    float score = p_hat;
+    float rnd = rand_f32(seed);
+    if ((rnd * sum_mc) < (p_hat * 21.0f)) {
+        if (near_zero(len(light_dir(state, x1)))) return state;
+        state.num_samples = min(state.num_samples + 1u, 1024u);
+        float alpha = state.num_samples == 1u ? 1.0f : fmaxf(1.0f / __uint2float_rn(state.num_samples), 0.01f) * confidence;
+        state.weight_sum = mixf(state.weight_sum, score, alpha);
+        state.light = mix3(state.light, x2 * score, alpha);
+        v3 mean = normalize(light_dir(state, x1));
+        state.mean_cosine = mixf(state.mean_cosine, score * dot(normalize(x2 - x1), mean), alpha);
+    }
+    return state;
+}
+
+}  // namespace lam

@@ -1,0 +1,342 @@
+// traverse.cuh - two-level compressed-BVH8 traversal with the watertight triangle test.
+//
+// Replaces the driver ray query used by ray_hit (src/path_tracing/general.wesl:1053-1078):
+// RayDesc(flags 0, cull mask 0xFF, T_MIN, T_MAX, origin, direction), committed closest hit.
+// Contract (identical to the CPU oracle's):
+//   * hit iff tmin < t < tmax; no face culling; opaque geometry commits without a callback;
+//     non-opaque geometry runs the reference's alpha test (general.wesl:1059-1067);
+//   * per triangle: Woop-Benthin-Wald watertight test in f32 with this exact operation order
+//     (explicit __f*_rn intrinsics, never contracted) and an FP64 recomputation of the three
+//     edge functions when any is exactly zero;
+//   * ties in t go to the lowest (instance, primitive) pair;
+//   * instances are entered with the f32 object-space ray o' = M^-1 o, d' = M^-1 d (fixed fma order).
+// The box test evaluates each slab plane as one FMA against the node's quantization grid; the
+// far distance is scaled by (1 + 2^-20) and child boxes carry one grid step of outward padding,
+// which together cover the f32 rounding of the slab distances.
+#pragma once
+#include "device_math.cuh"
+#include "scene.h"
+
+namespace lam {
+
+constexpr int TRAVERSAL_STACK = 32;
+constexpr uint32_t NO_HIT = 0xFFFFFFFFu;
+enum : uint32_t { ERR_STACK_OVERFLOW = 1u };
+
+struct TravRay {
+    float3 o, d, inv;
+    uint32_t oct;
+    int kx, ky, kz;
+    float Sx, Sy, Sz;
+};
+
+LAM_DEV float sel3(int k, float x, float y, float z) { return k == 0 ? x : (k == 1 ? y : z); }
+
+LAM_DEV float safe_rcp(float x) {
+    float y = fabsf(x) < 1e-30f ? copysignf(1e-30f, x) : x;
+    return __frcp_rn(y);
+}
+
+LAM_DEV void setup_ray(TravRay& r, float3 o, float3 d) {
+    r.o = o;
+    r.d = d;
+    r.inv = make_float3(safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z));
+    r.oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+    float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    int kz = 0;
+    float m = ax;
+    if (ay > m) { kz = 1; m = ay; }
+    if (az > m) kz = 2;
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    float dz = sel3(kz, d.x, d.y, d.z);
+    if (dz < 0.0f) { int t = kx; kx = ky; ky = t; }
+    r.kx = kx; r.ky = ky; r.kz = kz;
+    r.Sx = __fdiv_rn(sel3(kx, d.x, d.y, d.z), dz);
+    r.Sy = __fdiv_rn(sel3(ky, d.x, d.y, d.z), dz);
+    r.Sz = __fdiv_rn(1.0f, dz);
+}
+
+LAM_DEV void object_ray(const float* m, float3 o, float3 d, float3* oo, float3* od) {
+    oo->x = __fmaf_rn(m[0], o.x, __fmaf_rn(m[1], o.y, __fmaf_rn(m[2], o.z, m[3])));
+    oo->y = __fmaf_rn(m[4], o.x, __fmaf_rn(m[5], o.y, __fmaf_rn(m[6], o.z, m[7])));
+    oo->z = __fmaf_rn(m[8], o.x, __fmaf_rn(m[9], o.y, __fmaf_rn(m[10], o.z, m[11])));
+    od->x = __fmaf_rn(m[0], d.x, __fmaf_rn(m[1], d.y, __fmul_rn(m[2], d.z)));
+    od->y = __fmaf_rn(m[4], d.x, __fmaf_rn(m[5], d.y, __fmul_rn(m[6], d.z)));
+    od->z = __fmaf_rn(m[8], d.x, __fmaf_rn(m[9], d.y, __fmul_rn(m[10], d.z)));
+}
+
+// Watertight test (f32).  Returns true with the IEEE quotient t = T / det when the ray crosses
+// the triangle and t could beat `limit` (callers apply the exact tmin / limit / tie rules).
+LAM_DEV bool wbw_f32(const TravRay& r, float4 a, float4 b, float4 c, float limit, float* t_out) {
+    float Ax0 = __fsub_rn(a.x, r.o.x), Ay0 = __fsub_rn(a.y, r.o.y), Az0 = __fsub_rn(a.z, r.o.z);
+    float Bx0 = __fsub_rn(b.x, r.o.x), By0 = __fsub_rn(b.y, r.o.y), Bz0 = __fsub_rn(b.z, r.o.z);
+    float Cx0 = __fsub_rn(c.x, r.o.x), Cy0 = __fsub_rn(c.y, r.o.y), Cz0 = __fsub_rn(c.z, r.o.z);
+    float Akx = sel3(r.kx, Ax0, Ay0, Az0), Aky = sel3(r.ky, Ax0, Ay0, Az0), Akz = sel3(r.kz, Ax0, Ay0, Az0);
+    float Bkx = sel3(r.kx, Bx0, By0, Bz0), Bky = sel3(r.ky, Bx0, By0, Bz0), Bkz = sel3(r.kz, Bx0, By0, Bz0);
+    float Ckx = sel3(r.kx, Cx0, Cy0, Cz0), Cky = sel3(r.ky, Cx0, Cy0, Cz0), Ckz = sel3(r.kz, Cx0, Cy0, Cz0);
+    float Ax = __fmaf_rn(-r.Sx, Akz, Akx), Ay = __fmaf_rn(-r.Sy, Akz, Aky);
+    float Bx = __fmaf_rn(-r.Sx, Bkz, Bkx), By = __fmaf_rn(-r.Sy, Bkz, Bky);
+    float Cx = __fmaf_rn(-r.Sx, Ckz, Ckx), Cy = __fmaf_rn(-r.Sy, Ckz, Cky);
+    float U = __fmaf_rn(Cx, By, -__fmul_rn(Cy, Bx));
+    float V = __fmaf_rn(Ax, Cy, -__fmul_rn(Ay, Cx));
+    float W = __fmaf_rn(Bx, Ay, -__fmul_rn(By, Ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = __double2float_rn(__dsub_rn(__dmul_rn((double)Cx, (double)By), __dmul_rn((double)Cy, (double)Bx)));
+        V = __double2float_rn(__dsub_rn(__dmul_rn((double)Ax, (double)Cy), __dmul_rn((double)Ay, (double)Cx)));
+        W = __double2float_rn(__dsub_rn(__dmul_rn((double)Bx, (double)Ay), __dmul_rn((double)By, (double)Ax)));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    float det = __fadd_rn(__fadd_rn(U, V), W);
+    if (det == 0.0f) return false;
+    float Az = __fmul_rn(r.Sz, Akz), Bz = __fmul_rn(r.Sz, Bkz), Cz = __fmul_rn(r.Sz, Ckz);
+    float T = __fmaf_rn(U, Az, __fmaf_rn(V, Bz, __fmul_rn(W, Cz)));
+    // conservative early out: |T / det| certainly above the current limit
+    if (fabsf(T) > __fmul_rn(fabsf(det), limit) * 1.00000095367431640625f) return false;
+    *t_out = __fdiv_rn(T, det);
+    return true;
+}
+
+// FP64 re-evaluation of the committed hit (same formulas as the oracle, never contracted).
+LAM_DEV void wbw_f64(float3 of, float3 df, float4 p0, float4 p1, float4 p2, float* t, float* u, float* v,
+                     bool* front) {
+    TravRay sel;
+    // only the axis selection of setup_ray is needed
+    {
+        float ax = fabsf(df.x), ay = fabsf(df.y), az = fabsf(df.z);
+        int kz = 0;
+        float m = ax;
+        if (ay > m) { kz = 1; m = ay; }
+        if (az > m) kz = 2;
+        int kx = kz + 1 == 3 ? 0 : kz + 1;
+        int ky = kx + 1 == 3 ? 0 : kx + 1;
+        if (sel3(kz, df.x, df.y, df.z) < 0.0f) { int tt = kx; kx = ky; ky = tt; }
+        sel.kx = kx; sel.ky = ky; sel.kz = kz;
+    }
+    double o[3] = {of.x, of.y, of.z}, d[3] = {df.x, df.y, df.z};
+    double P0[3] = {p0.x, p0.y, p0.z}, P1[3] = {p1.x, p1.y, p1.z}, P2[3] = {p2.x, p2.y, p2.z};
+    double a[3], b[3], c[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        a[k] = __dsub_rn(P0[k], o[k]);
+        b[k] = __dsub_rn(P1[k], o[k]);
+        c[k] = __dsub_rn(P2[k], o[k]);
+    }
+    const int kx = sel.kx, ky = sel.ky, kz = sel.kz;
+    double dkx = kx == 0 ? d[0] : (kx == 1 ? d[1] : d[2]);
+    double dky = ky == 0 ? d[0] : (ky == 1 ? d[1] : d[2]);
+    double dkz = kz == 0 ? d[0] : (kz == 1 ? d[1] : d[2]);
+    auto pick = [&](const double* q, int k) { return k == 0 ? q[0] : (k == 1 ? q[1] : q[2]); };
+    double Sx = __ddiv_rn(dkx, dkz), Sy = __ddiv_rn(dky, dkz), Sz = __ddiv_rn(1.0, dkz);
+    double Ax = __dsub_rn(pick(a, kx), __dmul_rn(Sx, pick(a, kz))), Ay = __dsub_rn(pick(a, ky), __dmul_rn(Sy, pick(a, kz)));
+    double Bx = __dsub_rn(pick(b, kx), __dmul_rn(Sx, pick(b, kz))), By = __dsub_rn(pick(b, ky), __dmul_rn(Sy, pick(b, kz)));
+    double Cx = __dsub_rn(pick(c, kx), __dmul_rn(Sx, pick(c, kz))), Cy = __dsub_rn(pick(c, ky), __dmul_rn(Sy, pick(c, kz)));
+    double U = __dsub_rn(__dmul_rn(Cx, By), __dmul_rn(Cy, Bx));
+    double V = __dsub_rn(__dmul_rn(Ax, Cy), __dmul_rn(Ay, Cx));
+    double W = __dsub_rn(__dmul_rn(Bx, Ay), __dmul_rn(By, Ax));
+    double det = __dadd_rn(__dadd_rn(U, V), W);
+    double Az = __dmul_rn(Sz, pick(a, kz)), Bz = __dmul_rn(Sz, pick(b, kz)), Cz = __dmul_rn(Sz, pick(c, kz));
+    double T = __dadd_rn(__dadd_rn(__dmul_rn(U, Az), __dmul_rn(V, Bz)), __dmul_rn(W, Cz));
+    *t = __double2float_rn(__ddiv_rn(T, det));
+    *u = __double2float_rn(__ddiv_rn(V, det));
+    *v = __double2float_rn(__ddiv_rn(W, det));
+    double e1[3] = {__dsub_rn(P1[0], P0[0]), __dsub_rn(P1[1], P0[1]), __dsub_rn(P1[2], P0[2])};
+    double e2[3] = {__dsub_rn(P2[0], P0[0]), __dsub_rn(P2[1], P0[1]), __dsub_rn(P2[2], P0[2])};
+    double n0 = __dsub_rn(__dmul_rn(e1[1], e2[2]), __dmul_rn(e1[2], e2[1]));
+    double n1 = __dsub_rn(__dmul_rn(e1[2], e2[0]), __dmul_rn(e1[0], e2[2]));
+    double n2 = __dsub_rn(__dmul_rn(e1[0], e2[1]), __dmul_rn(e1[1], e2[0]));
+    double nd = __dadd_rn(__dadd_rn(__dmul_rn(n0, d[0]), __dmul_rn(n1, d[1])), __dmul_rn(n2, d[2]));
+    *front = nd < 0.0;
+}
+
+// One quantized child coordinate as an exact float (byte k of w).
+LAM_DEV float qbyte(uint32_t w, uint32_t k) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + k)) - 8388608.0f;
+}
+
+// Intersects the 8 children of one node.  Outputs the node group (child_base, internal hits in
+// bits 24..31 in octant order | imask) and the leaf group (leaf_base, item hits in bits 0..23).
+LAM_DEV void intersect_node(const uint4* __restrict__ np, const TravRay& r, float tmin, float tmax, uint2& ng,
+                            uint2& tg) {
+    const uint4 n0 = np[0], n1 = np[1], n2 = np[2], n3 = np[3], n4 = np[4];
+    const float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
+    const uint32_t imask = n0.w >> 24;
+    const float sx = __uint_as_float((n0.w & 0xFFu) << 23);
+    const float sy = __uint_as_float(((n0.w >> 8) & 0xFFu) << 23);
+    const float sz = __uint_as_float(((n0.w >> 16) & 0xFFu) << 23);
+    const float adx = __fmul_rn(sx, r.inv.x), ady = __fmul_rn(sy, r.inv.y), adz = __fmul_rn(sz, r.inv.z);
+    const float aox = __fmul_rn(__fsub_rn(px, r.o.x), r.inv.x);
+    const float aoy = __fmul_rn(__fsub_rn(py, r.o.y), r.inv.y);
+    const float aoz = __fmul_rn(__fsub_rn(pz, r.o.z), r.inv.z);
+    // near plane = lo plane when the inverse direction is positive
+    const bool fx = r.inv.x < 0.0f, fy = r.inv.y < 0.0f, fz = r.inv.z < 0.0f;
+    const uint32_t nx0 = fx ? n3.z : n2.x, nx1 = fx ? n3.w : n2.y, fx0 = fx ? n2.x : n3.z, fx1 = fx ? n2.y : n3.w;
+    const uint32_t ny0 = fy ? n4.x : n2.z, ny1 = fy ? n4.y : n2.w, fy0 = fy ? n2.z : n4.x, fy1 = fy ? n2.w : n4.y;
+    const uint32_t nz0 = fz ? n4.z : n3.x, nz1 = fz ? n4.w : n3.y, fz0 = fz ? n3.x : n4.z, fz1 = fz ? n3.y : n4.w;
+    uint32_t node_hits = 0u, leaf_hits = 0u;
+#pragma unroll
+    for (uint32_t i = 0; i < 8; ++i) {
+        const uint32_t k = i & 3u;
+        const float tnx = __fmaf_rn(qbyte(i < 4 ? nx0 : nx1, k), adx, aox);
+        const float tny = __fmaf_rn(qbyte(i < 4 ? ny0 : ny1, k), ady, aoy);
+        const float tnz = __fmaf_rn(qbyte(i < 4 ? nz0 : nz1, k), adz, aoz);
+        const float tfx = __fmaf_rn(qbyte(i < 4 ? fx0 : fx1, k), adx, aox);
+        const float tfy = __fmaf_rn(qbyte(i < 4 ? fy0 : fy1, k), ady, aoy);
+        const float tfz = __fmaf_rn(qbyte(i < 4 ? fz0 : fz1, k), adz, aoz);
+        const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+        const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
+        if (tn <= tf * 1.00000095367431640625f) {
+            const uint32_t meta = ((i < 4 ? n1.z : n1.w) >> (8u * k)) & 0xFFu;
+            if (imask & (1u << i)) {
+                node_hits |= 1u << (i ^ r.oct);
+            } else {
+                leaf_hits |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
+            }
+        }
+    }
+    ng = make_uint2(n1.x, (node_hits << 24) | imask);
+    tg = make_uint2(n1.y, leaf_hits);
+}
+
+struct TraceResult {
+    uint32_t tri;   // global triangle slot, NO_HIT if none
+    uint32_t inst;
+    uint32_t prim;
+    float t;        // f32 watertight distance
+};
+
+// Alpha-test callback for non-opaque geometry: candidate accepted unless the diffuse texel's
+// alpha is near zero, transparent materials always accepted (general.wesl:1059-1067).
+LAM_DEV bool alpha_accept(const DevScene& S, uint32_t inst, uint32_t prim, float bu, float bv);
+
+template <bool ANY, bool ALPHA>
+LAM_DEV TraceResult trace_ray(const DevScene& S, const uint4* __restrict__ tlas_nodes,
+                              const DevInstance* __restrict__ insts, float3 wo, float3 wd, float tmin, float tmax,
+                              uint32_t& err) {
+    TraceResult res;
+    res.tri = NO_HIT;
+    res.inst = NO_HIT;
+    res.prim = NO_HIT;
+    res.t = tmax;
+    if (S.tlas_node_count == 0u) return res;
+    float best_t = tmax;
+    TravRay R;
+    setup_ray(R, wo, wd);
+    uint2 stack[TRAVERSAL_STACK];
+    int sp = 0;
+    int blas_base = -1;
+    uint32_t cur_inst = 0u, cur_flags = 0u;
+    const uint4* __restrict__ nodes = tlas_nodes;
+    uint2 ng = make_uint2(0u, (1u << (24u + R.oct)) | 1u);
+    uint2 tg = make_uint2(0u, 0u);
+    for (;;) {
+        if (ng.y > 0x00FFFFFFu) {
+            const uint32_t k = __ffs(ng.y >> 24) - 1u;
+            ng.y &= ~(1u << (24u + k));
+            const uint32_t slot = k ^ R.oct;
+            const uint32_t child = ng.x + __popc(ng.y & ((1u << slot) - 1u) & 0xFFu);
+            if (ng.y > 0x00FFFFFFu) {
+                if (sp < TRAVERSAL_STACK) stack[sp++] = ng;
+                else err |= ERR_STACK_OVERFLOW;
+            }
+            intersect_node(nodes + 5u * child, R, tmin, best_t, ng, tg);
+        } else {
+            tg = ng;
+            ng = make_uint2(0u, 0u);
+        }
+        while (tg.y != 0u) {
+            const uint32_t k = __ffs(tg.y) - 1u;
+            tg.y &= tg.y - 1u;
+            const uint32_t item = tg.x + k;
+            if (blas_base < 0) {
+                const uint32_t id = __ldg(S.tlas_items + item);
+                const DevInstance& I = insts[id];
+                const uint32_t flags = I.flags;
+                const uint32_t root = I.blas_root;
+                if (!(flags & INST_VISIBLE) || root == NO_HIT) continue;
+                if (tg.y != 0u) {
+                    if (sp < TRAVERSAL_STACK) stack[sp++] = tg;
+                    else err |= ERR_STACK_OVERFLOW;
+                }
+                if (ng.y > 0x00FFFFFFu) {
+                    if (sp < TRAVERSAL_STACK) stack[sp++] = ng;
+                    else err |= ERR_STACK_OVERFLOW;
+                }
+                blas_base = sp;
+                cur_inst = id;
+                cur_flags = flags;
+                nodes = S.blas_nodes;
+                float m[12];
+#pragma unroll
+                for (int q = 0; q < 12; ++q) m[q] = I.inv[q];
+                float3 oo, od;
+                object_ray(m, wo, wd, &oo, &od);
+                setup_ray(R, oo, od);
+                ng = make_uint2(root, (1u << (24u + R.oct)) | 1u);
+                tg = make_uint2(0u, 0u);
+                break;
+            }
+            const float4* tp = S.tris + 3u * item;
+            const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+            float t;
+            if (!wbw_f32(R, a, b, c, best_t, &t)) continue;
+            const uint32_t prim = __float_as_uint(a.w);
+            bool better = t > tmin && (t < best_t || (t == best_t && res.tri != NO_HIT &&
+                                                      (cur_inst < res.inst || (cur_inst == res.inst && prim < res.prim))));
+            if (!better) continue;
+            if (ALPHA && !(cur_flags & INST_OPAQUE)) {
+                float rt, ru, rv;
+                bool fr;
+                wbw_f64(R.o, R.d, a, b, c, &rt, &ru, &rv, &fr);
+                if (!alpha_accept(S, cur_inst, prim, ru, rv)) continue;
+            }
+            best_t = t;
+            res.tri = item;
+            res.inst = cur_inst;
+            res.prim = prim;
+            if (ANY) {
+                res.t = best_t;
+                return res;
+            }
+        }
+        if (ng.y <= 0x00FFFFFFu && tg.y == 0u) {
+            if (blas_base >= 0 && sp == blas_base) {
+                blas_base = -1;
+                nodes = tlas_nodes;
+                setup_ray(R, wo, wd);
+            }
+            if (sp == 0) break;
+            ng = stack[--sp];
+        }
+    }
+    res.t = best_t;
+    return res;
+}
+
+constexpr int TRACE_BLOCK = 128;
+constexpr uint32_t SMEM_TLAS_NODES = 64;   // TLAS staged in shared memory when it fits
+constexpr uint32_t SMEM_INSTANCES = 128;
+
+struct TraceSmem {
+    uint4 tlas[SMEM_TLAS_NODES * 5];
+    DevInstance inst[SMEM_INSTANCES];
+};
+
+// Copies the TLAS nodes and instance records into shared memory when they fit (they are read
+// by every ray); returns the pointers the traversal should use.
+LAM_DEV void stage_tlas(const DevScene& S, TraceSmem& sm, const uint4*& tl, const DevInstance*& in) {
+    tl = S.tlas_nodes;
+    in = S.inst;
+    const bool fit = S.tlas_node_count <= SMEM_TLAS_NODES && S.instance_count <= SMEM_INSTANCES;
+    if (fit) {
+        for (uint32_t i = threadIdx.x; i < S.tlas_node_count * 5u; i += blockDim.x) sm.tlas[i] = S.tlas_nodes[i];
+        const uint4* src = reinterpret_cast<const uint4*>(S.inst);
+        uint4* dst = reinterpret_cast<uint4*>(sm.inst);
+        for (uint32_t i = threadIdx.x; i < S.instance_count * 4u; i += blockDim.x) dst[i] = src[i];
+        tl = sm.tlas;
+        in = sm.inst;
+    }
+    __syncthreads();
+}
+
+}  // namespace lam

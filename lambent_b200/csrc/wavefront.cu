@@ -1,0 +1,1125 @@
+// wavefront.cu - rt_main of the reference (src/path_tracing/general.wesl:506-975) as a wavefront:
+//
+//   generate   one thread per pixel: seed chain, camera ray per sample of the wave
+//   extend     persistent warps: closest hit for every queued path (traverse.cuh)
+//   shade      one bounce of rt_sample for every queued path; survivors are appended to the next queue
+//   accumulate one thread per pixel: per-sample colours summed in sample order, reservoirs, outputs
+//   shuffle    (Markov guiding) the per-sample subgroup shuffle of the tentative chains
+//
+// Path state lives in HBM as structure-of-arrays indexed by path id = sample_in_wave * pixels + pixel.
+// A wave holds `spp_wave` samples of every pixel; samples of one pixel are independent except through
+// the Markov chains and per-sample ReSTIR, which therefore run one sample per wave.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "guide.cuh"
+#include "materials.cuh"
+#include "scene.h"
+#include "tracer.h"
+#include "traverse.cuh"
+
+namespace lam {
+
+constexpr int WAVE_BLOCK = 128;
+
+struct Isect {
+    v3 color;
+    float t;
+    v3 emission;
+    uint32_t ty;
+    v3 normal;
+    bool front_face;
+    v3 tangent;
+    float2 roughness, roughness_transparent;
+    float ior_low, ior_high;
+};
+
+// ray_hit's post-query part (general.wesl:1080-1137) for a committed triangle.
+LAM_DEV void make_isect(const DevScene& S, const DevInstance* insts, uint2 hit, float3 o, float3 d, Isect& r) {
+    float m[12];
+#pragma unroll
+    for (int q = 0; q < 12; ++q) m[q] = insts[hit.y].inv[q];
+    float3 oo, od;
+    object_ray(m, o, d, &oo, &od);
+    const float4* tp = S.tris + 3u * hit.x;
+    const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+    float t, bu, bv;
+    bool front;
+    wbw_f64(oo, od, a, b, c, &t, &bu, &bv, &front);
+    r.t = t;
+    r.front_face = front;
+    const uint32_t prim = __float_as_uint(a.w);
+    const lam_material mt = load_material(S, hit.y, prim);
+    const uint32_t idx_d = mt.tex_idx_diffuse_emission & 0xFFFFu, idx_e = mt.tex_idx_diffuse_emission >> 16;
+    const uint32_t idx_a = mt.tex_idx_attributes_ty & 0xFFFFu;
+    r.ty = mt.tex_idx_attributes_ty >> 16;
+    float2 ri = unpack2x16float(mt.refractive_index);
+    r.ior_low = ri.x;
+    r.ior_high = ri.y;
+    v3 v0 = mk(a.x, a.y, a.z), v1 = mk(b.x, b.y, b.z), v2 = mk(c.x, c.y, c.z);
+    v3 tg = normalize(v0 - v1);
+    {
+        float ax = fabsf(tg.x), ay = fabsf(tg.y), az = fabsf(tg.z);
+        bool xl = ax > ay && ax > az, yl = ay > ax && ay > az;
+        bool rev = xl ? tg.x < 0.0f : (yl ? tg.y < 0.0f : tg.z < 0.0f);
+        if (rev) tg = -tg;
+    }
+    v3 n = normalize(cross(tg, v0 - v2));
+    v3 dw = mk(d.x, d.y, d.z);
+    r.normal = dot(dw, n) > 0.0f ? -n : n;
+    r.tangent = tg;
+    float2 uv = hit_uv(mt, bu, bv);
+    float4 dc = tex_sample(S, S.diffuse_first, S.diffuse_count, idx_d, uv.x, uv.y);
+    float4 rc = recolour_load(S, mt.tex_pos_recolour & 0xFFFFu, mt.tex_pos_recolour >> 16);
+    v3 diffuse = mk(dc.x, dc.y, dc.z) * mk(rc.x, rc.y, rc.z);
+    r.color = diffuse;
+    float es_x = __uint_as_float((mt.emission_scale & 0xFFFFu) << 16);
+    float es_y = __uint_as_float((mt.emission_scale >> 16) << 16);
+    r.emission = splat(0.0f);
+    if (idx_e != 0xFFFFu) {
+        float4 ec = tex_sample(S, S.emission_first, S.emission_count, idx_e, uv.x, uv.y);
+        r.emission = mk(ec.x, ec.y, ec.z) * es_x;
+    }
+    r.emission = r.emission + diffuse * es_y;
+    r.roughness = make_float2(0.0f, 0.0f);
+    r.roughness_transparent = make_float2(0.0f, 0.0f);
+    if (idx_a != 0xFFFFu) {
+        float4 at = tex_sample(S, S.attr_first, S.attr_count, idx_a, uv.x, uv.y);
+        r.roughness = make_float2(at.x, at.y);
+        r.roughness_transparent = make_float2(at.z, at.w);
+    }
+}
+
+// ---------------------------------------------------------------- BSDF helpers (general.wesl:1206-1289)
+LAM_DEV v3 to_onb(v3 src, v3 up, v3 tangent) {
+    v3 s = tangent, t = cross(up, s);
+    v3 inv_s = cross(up, t), inv_up = cross(t, s), inv_t = cross(s, up);
+    return fma3(splat(src.x), inv_s, fma3(splat(src.y), inv_up, inv_t * src.z));
+}
+LAM_DEV v3 from_onb(v3 src, v3 up, v3 tangent) {
+    v3 s = tangent, t = cross(up, s);
+    return fma3(splat(src.x), s, fma3(splat(src.y), up, t * src.z));
+}
+LAM_DEV v3 from_onb_no_tangent(v3 src, v3 up) {
+    v3 other = near_zero(up.x) ? mk(1.0f, 0.0f, 0.0f) : mk(0.0f, 1.0f, 0.0f);
+    return from_onb(src, up, normalize(cross(up, other)));
+}
+LAM_DEV v3 cosine_hemisphere(uint32_t seed, v3 n, v3 t) {
+    float r1 = rand_f32(seed), r2 = rand_f32(seed + 1u);
+    float phi = TAU_F * r1;
+    v3 h = mk(cosf(phi) * sqrtf(r2), sqrtf(1.0f - r2), sinf(phi) * sqrtf(r2));
+    return from_onb(h, n, t);
+}
+LAM_DEV v3 sample_vndf_ggx(uint32_t seed, v3 view, float2 rough) {
+    float u1 = rand_f32(seed), u2 = rand_f32(seed + 1u);
+    v3 in = mk(view.x * rough.x, view.y, view.z * rough.y);
+    if (v3_near_zero(in)) in = mk(0.0f, -1.0f, 0.0f);
+    v3 wi = normalize(in);
+    float phi = TAU_F * u1;
+    float y = fmaf(1.0f - u2, 1.0f + wi.y, -wi.y);
+    float st = sqrtf(clampf(fmaf(y, -y, 1.0f), 0.0f, 1.0f));
+    v3 wm = mk(st * cosf(phi), y, st * sinf(phi)) + wi;
+    v3 out = mk(wm.x * rough.x, wm.y, wm.z * rough.y);
+    if (v3_near_zero(out)) out = mk(0.0f, 1.0f, 0.0f);
+    return normalize(out);
+}
+LAM_DEV float reflectance(float c, float ri) {
+    float r0 = (1.0f - ri) / (1.0f + ri);
+    float r0s = r0 * r0;
+    return fmaf(1.0f - r0s, powf(1.0f - c, 5.0f), r0s);
+}
+LAM_DEV v3 oren_nayar(v3 incoming, v3 reflected, float rough, v3 color) {
+    float rr = rough * HALF_PI_F;
+    float rr2 = rr * rr;
+    v3 a = fma3(color * 0.17f, splat(rr2 / (rr2 + 0.13f)), splat(1.0f - (0.5f * (rr2 / (rr2 + 0.33f)))));
+    float b = 0.45f * (rr2 / (rr2 + 0.09f));
+    float s = fmaf(-reflected.y, incoming.y, dot(reflected, incoming));
+    float t = 1.0f;
+    if (s > 0.0f) {
+        t = fmaxf(reflected.y, incoming.y);
+        if (near_zero(t)) t = 0.001f;
+    }
+    return fma3(splat(b), splat(s / t), a);
+}
+LAM_DEV float g_lobe(float x, float u, float t1, float t2) {
+    float tau = x < u ? t1 : t2;
+    float dd = x - u;
+    return expf(-((dd * dd) * (tau * tau)) * 0.5f);
+}
+
+// ---------------------------------------------------------------- wave buffers
+struct WaveBuffers {
+    uint32_t width = 0, height = 0, npix = 0, spp_wave = 0;
+    uint64_t paths = 0;
+    bool full = false, guide = false;
+    float4 *ray_o = nullptr, *ray_d = nullptr;
+    uint2* hit = nullptr;
+    uint32_t *queue0 = nullptr, *queue1 = nullptr;
+    float4 *thr = nullptr, *acc = nullptr;
+    float* brdf = nullptr;
+    uint32_t *seed = nullptr, *flags = nullptr;
+    // restir / guide state
+    float4 *ort = nullptr, *orad = nullptr, *ppoint = nullptr, *pnormal = nullptr, *vpoint = nullptr,
+           *vnormal = nullptr, *lnormal = nullptr, *ldir = nullptr;
+    // per pixel
+    float4 *pix_color = nullptr, *pix_orad = nullptr, *pix_emission = nullptr, *pix_albedo = nullptr;
+    lam_markov_chain *tent_snap = nullptr, *tent_live = nullptr;
+    uint32_t* ctr = nullptr;  // [0..1] queue counts, [2..3] work counters, [4] error flags
+    std::vector<void*> allocs;
+    int sms = 148, grid_extend = 0, grid_shade = 0;
+};
+
+static void free_wave(WaveBuffers* w) {
+    if (!w) return;
+    for (void* p : w->allocs) cudaFree(p);
+    delete w;
+}
+
+template <class T>
+static int walloc(WaveBuffers* w, T** p, size_t count) {
+    *p = nullptr;
+    if (!count) return LAM_OK;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess) return cuda_error(e, "cudaMalloc (wavefront state)");
+    w->allocs.push_back(*p);
+    return LAM_OK;
+}
+
+// ---------------------------------------------------------------- kernel arguments
+struct Args {
+    DevScene S;
+    lam_camera cam;
+    uint32_t width, height, npix, samples, max_depth, restir, seed_offset;
+    float tmin, tmax;
+    uint32_t wave_first, wave_count;
+    // wave buffers
+    float4 *ray_o, *ray_d;
+    uint2* hit;
+    uint32_t *q_in, *q_out;
+    uint32_t *count_in, *count_out, *work;
+    uint32_t* err;
+    unsigned long long* segments;
+    float4 *thr, *acc;
+    float* brdf;
+    uint32_t *seed, *flags;
+    float4 *ort, *orad, *ppoint, *pnormal, *vpoint, *vnormal, *lnormal, *ldir;
+    float4 *pix_color, *pix_orad, *pix_emission, *pix_albedo;
+    lam_markov_chain *tent_snap, *tent_live;
+    // data buffers
+    const lam_markov_chain* old_chains;
+    lam_markov_chain* chains;
+    uint64_t chains_len, old_chains_len;
+    uint32_t* world;
+    const uint32_t* old_world;
+    uint64_t world_len;
+    lam_reservoir* reservoirs;
+    lam_info* info;
+    uint32_t* pixel_seed;
+    // outputs
+    float4 *out_color, *out_normal, *out_albedo;
+    v3 camera_pos;
+};
+
+LAM_DEV void create_ray(const Args& A, uint32_t x, uint32_t y, v3* o, v3* d) {
+    float hx = __uint2float_rn(A.width) / 2.0f, hy = __uint2float_rn(A.height) / 2.0f;
+    float nx = (__uint2float_rn(x) / hx) - 1.0f, ny = (__uint2float_rn(y) / hy) - 1.0f;
+    float v[4] = {nx, -ny, 1.0f, 1.0f};
+    const float* P = A.cam.projection_inverse;
+    float q[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q[i] = P[i] * v[0] + P[4 + i] * v[1] + P[8 + i] * v[2] + P[12 + i] * v[3];
+    float l = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q[i] = q[i] / l;
+    const float* V = A.cam.view_inverse;
+    *d = mk(V[0] * q[0] + V[4] * q[1] + V[8] * q[2] + V[12] * 0.0f, V[1] * q[0] + V[5] * q[1] + V[9] * q[2] + V[13] * 0.0f,
+            V[2] * q[0] + V[6] * q[1] + V[10] * q[2] + V[14] * 0.0f);
+    *o = A.camera_pos;
+}
+
+LAM_DEV uint32_t advance_fill_seed(uint32_t s) {
+#pragma unroll 4
+    for (int i = 0; i < 12; ++i) {
+        s = rand_u32(s);
+        s = rand_u32(s);
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------- generate
+__global__ void __launch_bounds__(WAVE_BLOCK) generate_kernel(Args A) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p == 0) *A.count_in = A.npix * A.wave_count;
+    if (p >= A.npix) return;
+    const uint32_t x = p % A.width, y = p / A.width;
+    uint32_t st;
+    if (A.wave_first == 0u) {
+        st = rand_u32(x * y) + A.seed_offset + y;
+        A.pix_color[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (A.pix_orad) A.pix_orad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (A.tent_live) {
+            MC t = (A.old_chains && p < A.old_chains_len) ? mc_load(A.old_chains + p) : mc_zero();
+            mc_store(A.tent_live + p, t);
+            mc_store(A.tent_snap + p, t);
+        }
+        if (A.reservoirs && A.restir == LAM_RESTIR_PER_SAMPLE) A.reservoirs[p] = lam_reservoir{};
+    } else {
+        st = A.pixel_seed[p];
+        if (A.tent_live) mc_store(A.tent_live + p, mc_load(A.tent_snap + p));
+    }
+    v3 o, d;
+    create_ray(A, x, y, &o, &d);
+    for (uint32_t j = 0; j < A.wave_count; ++j) {
+        const uint32_t path = j * A.npix + p;
+        const uint32_t fill_seed = st;
+        st = advance_fill_seed(st);
+        A.seed[path] = st;
+        A.ray_o[path] = make_float4(o.x, o.y, o.z, 0.0f);
+        A.ray_d[path] = make_float4(d.x, d.y, d.z, 0.0f);
+        A.thr[path] = make_float4(1.0f, 1.0f, 1.0f, -1.0f);
+        A.acc[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        A.brdf[path] = 0.0f;
+        A.flags[path] = 0u;
+        if (A.ort) {
+            A.ort[path] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+            A.orad[path] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+            A.ppoint[path] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(TY_SKY));
+            A.pnormal[path] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(fill_seed));
+            A.vpoint[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            A.vnormal[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        if (A.lnormal) {
+            A.lnormal[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            A.ldir[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        A.q_in[path] = path;
+        st = rand_u32(st);
+    }
+    A.pixel_seed[p] = st;
+}
+
+// ---------------------------------------------------------------- extend
+template <bool ALPHA>
+__global__ void __launch_bounds__(WAVE_BLOCK) extend_kernel(Args A) {
+    __shared__ TraceSmem sm;
+    const uint4* tl;
+    const DevInstance* in;
+    stage_tlas(A.S, sm, tl, in);
+    const uint32_t n = *A.count_in;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(A.segments, (unsigned long long)n);      // this render
+        atomicAdd(A.segments + 1, (unsigned long long)n);  // since the pipeline's buffers were created
+    }
+    uint32_t err = 0u;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(A.work, 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= n) break;
+        const uint32_t i = base + lane;
+        if (i >= n) continue;
+        const uint32_t path = A.q_in[i];
+        const float4 o4 = A.ray_o[path], d4 = A.ray_d[path];
+        TraceResult tr = trace_ray<false, ALPHA>(A.S, tl, in, make_float3(o4.x, o4.y, o4.z), make_float3(d4.x, d4.y, d4.z),
+                                                 A.tmin, A.tmax, err);
+        A.hit[path] = make_uint2(tr.tri, tr.inst);
+    }
+    if (err) atomicOr(A.err, err);
+}
+
+// ---------------------------------------------------------------- shade (one bounce of rt_sample)
+template <int Q, bool GUIDE>
+struct Shader {
+    LAM_DEV static v3 get_normal(v3 rd, v3 n, v3 t, uint32_t seed, float2 rough) {
+        if (Q == LAM_QUALITY_LOW) return n;
+        return from_onb(sample_vndf_ggx(seed, to_onb(rd, n, t), rough), n, t);
+    }
+    LAM_DEV static v3 make_diffuse(v3 hit_color, v3 rd, v3 n, v3 t, float rough, v3 new_dir) {
+        if (Q == LAM_QUALITY_LOW) return splat(1.0f);
+        return oren_nayar(to_onb(rd, n, t), new_dir, rough, hit_color);
+    }
+    // returns (weights.xyz, ior); picked_idx < 0 means "not picked yet"
+    LAM_DEV static float4 pick_ref_idx(float* picked_idx, float low, float high, uint32_t seed) {
+        if (Q == LAM_QUALITY_LOW) return make_float4(1.0f, 1.0f, 1.0f, low);
+        if (Q == LAM_QUALITY_MEDIUM) {
+            if (*picked_idx < 0.0f) *picked_idx = rand_f32(seed);
+            return make_float4(1.0f, 1.0f, 1.0f, mixf(low, high, *picked_idx));
+        }
+        if (*picked_idx < 0.0f) {
+            float pi = rand_f32(seed);
+            *picked_idx = pi;
+            float lambda = mixf(760.0f, 340.0f, pi);
+            float x = fmaf(1.056f, g_lobe(lambda, 599.8f, 0.0264f, 0.0323f),
+                           fmaf(0.362f, g_lobe(lambda, 442.0f, 0.0624f, 0.0374f), -(0.065f * g_lobe(lambda, 501.1f, 0.049f, 0.0382f))));
+            float y = fmaf(0.821f, g_lobe(lambda, 568.8f, 0.0213f, 0.0248f), 0.286f * g_lobe(lambda, 530.9f, 0.0613f, 0.0322f));
+            float z = fmaf(1.217f, g_lobe(lambda, 437.0f, 0.0845f, 0.0278f), 0.681f * g_lobe(lambda, 459.0f, 0.0385f, 0.0725f));
+            v3 rgb = mk(3.2406f, -0.9689f, 0.0557f) * x + mk(-1.5372f, 1.8758f, -0.204f) * y + mk(-0.4986f, 0.0415f, 1.057f) * z;
+            return make_float4(saturate(rgb.x) * 3.910f, saturate(rgb.y) * 4.411f, saturate(rgb.z) * 5.511f, mixf(low, high, pi));
+        }
+        return make_float4(1.0f, 1.0f, 1.0f, mixf(low, high, *picked_idx));
+    }
+};
+
+// 16 screen-space candidates of the sample (general.wesl:367-385), recomputed from the seed the
+// sample started its fill with.
+LAM_DEV void screen_candidates(const Args& A, uint32_t pixel, uint32_t fill_seed, MC* cand) {
+    const uint32_t x = pixel % A.width, y = pixel / A.width;
+    const uint32_t gbase = x & ~31u;
+    uint32_t s = fill_seed;
+    const uint32_t sub = rand_u32(s) % 32u;
+    MC sh = (gbase + sub < A.width) ? mc_load(A.tent_snap + (uint64_t)y * A.width + gbase + sub) : mc_zero();
+    for (int i = 0; i < 4; ++i) cand[i] = sh;
+    for (int i = 4; i < 16; ++i) {
+        uint32_t xr = rand_u32(s);
+        s = xr;
+        uint32_t yr = rand_u32(s);
+        s = yr;
+        int32_t dx = (int32_t)(xr % 91u) - 45, dy = (int32_t)(yr % 91u) - 45;
+        uint32_t nx = (uint32_t)((int32_t)x + dx), ny = (uint32_t)((int32_t)y + dy);
+        uint64_t idx = (uint32_t)(nx + ny * A.width);
+        if (A.old_chains && A.old_chains_len) {
+            idx = idx < A.old_chains_len ? idx : A.old_chains_len - 1;
+            cand[i] = mc_load(A.old_chains + idx);
+        } else {
+            cand[i] = mc_zero();
+        }
+    }
+}
+
+template <int Q, bool GUIDE>
+__global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(Args A) {
+    const uint32_t n = *A.count_in;
+    const uint32_t lane = threadIdx.x & 31u;
+    Grid G;
+    G.world = A.world;
+    G.old_world = A.old_world;
+    G.len = A.world_len;
+    G.camera_loc = A.camera_pos;
+    const bool rec = A.ort != nullptr;
+    for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;; base += gridDim.x * blockDim.x) {
+        if (base >= n) break;
+        const uint32_t i = base + lane;
+        bool cont = false;
+        uint32_t path = 0;
+        if (i < n) {
+            path = A.q_in[i];
+            const uint32_t pixel = path % A.npix;
+            const uint32_t sample_index = A.wave_first + path / A.npix;
+            const bool last_sample = sample_index + 1u == A.samples;
+            uint32_t fl = A.flags[path];
+            const uint32_t depth = fl & 0xFFu;
+            bool last_not_vmf = (fl >> 8) & 1u;
+            const float4 o4 = A.ray_o[path], d4 = A.ray_d[path];
+            v3 ro = mk(o4.x, o4.y, o4.z), rd = mk(d4.x, d4.y, d4.z);
+            float4 th = A.thr[path];
+            v3 color = mk(th.x, th.y, th.z);
+            float picked = th.w;
+            float4 ac = A.acc[path];
+            v3 scol = mk(ac.x, ac.y, ac.z);
+            float cached_pdf = ac.w, cached_brdf = A.brdf[path];
+            uint32_t seed = A.seed[path];
+            v3 orc = splat(1.0f), orad = splat(0.0f);
+            float sum_mc = 0.0f;
+            float4 pp = make_float4(0, 0, 0, 0), pn = make_float4(0, 0, 0, 0);
+            if (rec) {
+                float4 t0 = A.ort[path], t1 = A.orad[path];
+                orc = mk(t0.x, t0.y, t0.z);
+                sum_mc = t0.w;
+                orad = mk(t1.x, t1.y, t1.z);
+                pp = A.ppoint[path];
+                pn = A.pnormal[path];
+            }
+            v3 last_normal = splat(0.0f), last_dir = splat(0.0f);
+            if (GUIDE) {
+                float4 a = A.lnormal[path], b = A.ldir[path];
+                last_normal = mk(a.x, a.y, a.z);
+                last_dir = mk(b.x, b.y, b.z);
+            }
+            MC tentative = GUIDE ? mc_load(A.tent_live + pixel) : mc_zero();
+            const uint2 h = A.hit[path];
+            bool terminated = false;
+            if (h.x != NO_HIT) {
+                Isect is;
+                make_isect(A.S, A.S.inst, h, make_float3(ro.x, ro.y, ro.z), make_float3(rd.x, rd.y, rd.z), is);
+                v3 new_pos = fma3(rd, splat(is.t), ro);
+                if (depth != 0u) {
+                    v3 est = GUIDE ? grid_radiance(G, new_pos, is.normal, rd) : splat(0.0f);
+                    v3 rad_refl = strip_nan3(((is.color * est) * cached_brdf) / cached_pdf);
+                    v3 rad_out = (is.emission * cached_brdf) / cached_pdf;
+                    if (GUIDE) grid_add_radiance(G, ro, last_normal, last_dir, rad_out + rad_refl);
+                    float weight = len(rad_out + rad_refl);
+                    if (weight > 0.0f) {
+                        if (GUIDE) {
+                            MC st = update_chain(ro, new_pos, weight, seed, false, grid_load(G, ro, last_normal, last_dir, false),
+                                                 1.0f, sum_mc);
+                            grid_store(G, ro, last_normal, last_dir, st);
+                            tentative = update_chain(ro, new_pos, len(rad_out), seed, last_not_vmf, tentative,
+                                                     depth == 1u ? 1.0f : 0.5f, sum_mc);
+                        }
+                        seed++;
+                    }
+                }
+                last_normal = is.normal;
+                last_dir = rd;
+                last_not_vmf = false;
+                ro = new_pos;
+                if (depth == 0u) {
+                    if (rec) {
+                        pp = make_float4(ro.x, ro.y, ro.z, __uint_as_float(is.ty));
+                        pn = make_float4(is.normal.x, is.normal.y, is.normal.z, pn.w);
+                    }
+                    if (last_sample) {
+                        if (A.out_normal) A.out_normal[pixel] = make_float4(is.normal.x, is.normal.y, is.normal.z, 1.0f);
+                        if (A.out_albedo) A.out_albedo[pixel] = make_float4(is.color.x, is.color.y, is.color.z, 1.0f);
+                        if (A.pix_emission) {
+                            A.pix_emission[pixel] = make_float4(is.emission.x, is.emission.y, is.emission.z, 0.0f);
+                            A.pix_albedo[pixel] = make_float4(is.color.x, is.color.y, is.color.z, 0.0f);
+                        }
+                    }
+                } else if (depth == 1u && rec) {
+                    A.vpoint[path] = make_float4(ro.x, ro.y, ro.z, 0.0f);
+                    A.vnormal[path] = make_float4(is.normal.x, is.normal.y, is.normal.z, 0.0f);
+                }
+                scol = fma3(color, is.emission, scol);
+                if (depth != 0u) orad = fma3(orc, is.emission, orad);
+                v3 assign_normal = Shader<Q, GUIDE>::get_normal(rd, is.normal, is.tangent, seed, is.roughness);
+                v3 normal = Shader<Q, GUIDE>::get_normal(rd, is.normal, is.tangent, seed, is.roughness_transparent);
+                bool should_reflect = false;
+                seed += 1u;
+                float4 cri = Shader<Q, GUIDE>::pick_ref_idx(&picked, is.ior_low, is.ior_high, seed);
+                float ri = cri.w;
+                seed += 1u;
+                if (!(!is.front_face && is.ty == TY_TRANSPARENT)) ri = 1.0f / ri;
+                v3 cw = mk(cri.x, cri.y, cri.z);
+                color = color * cw;
+                orc = orc * cw;
+                if (ri != 1.0f) {
+                    float cos_theta = fminf(dot(-rd, normal), 1.0f);
+                    float sin_theta = sqrtf(1.0f - (cos_theta * cos_theta));
+                    bool cannot_refract = (ri * sin_theta) > 1.0f;
+                    float pdf = reflectance(cos_theta, ri);
+                    if (cannot_refract || (pdf > rand_f32(seed))) should_reflect = true;
+                    seed += 1u;
+                }
+                if (!should_reflect || is.ty == TY_TRANSPARENT) {
+                    color = color * is.color;
+                    if (depth != 0u) orc = orc * is.color;
+                }
+                if (!should_reflect) {
+                    normal = assign_normal;
+                    seed += 1u;
+                }
+                // fill_mc_world_space_states + resample_mcmm (general.wesl:389-425)
+                MC cand[NUM_RESAMPLES];
+                MC s = mc_zero();
+                if (GUIDE) {
+                    screen_candidates(A, pixel, __float_as_uint(pn.w), cand);
+                    for (int k = 16; k < 20; ++k) {
+                        bool rc = rand_f32(seed) < 0.7f;
+                        float jm = rc ? 0.75f : 1.0f;
+                        float j0 = rand_f32_ptr(&seed);
+                        float j1 = rand_f32_ptr(&seed);
+                        v3 jit = (mk(j0, 0.0f, j1) * 0.15000000596046448f) * jm;
+                        cand[k] = grid_load(G, ro + from_onb_no_tangent(jit, is.normal), is.normal, rd, rc);
+                        seed += 1u;
+                    }
+                    cand[20] = tentative;
+                    sum_mc = 0.0f;
+                    for (int k = 0; k < NUM_RESAMPLES; ++k) {
+                        seed = rand_u32(seed);
+                        sum_mc += cand[k].weight_sum;
+                        if (rand_f32(seed) * sum_mc < cand[k].weight_sum) s = cand[k];
+                        seed = rand_u32(seed);
+                    }
+                } else {
+                    for (int k = 16; k < 20; ++k) {
+                        seed = rand_u32(rand_u32(seed)) + 1u;
+                    }
+#pragma unroll 7
+                    for (int k = 0; k < NUM_RESAMPLES; ++k) seed = rand_u32(rand_u32(seed));
+                }
+                const bool reflecting = should_reflect || is.ty == TY_METALLIC;
+                if (!reflecting) {
+                    if (is.ty == TY_DIFFUSE) {
+                        v3 dir_cos = cosine_hemisphere(seed, is.normal, is.tangent);
+                        float cos_pdf = fmaxf(dot(dir_cos, is.normal) / PI_F, 0.0f);
+                        float theta = rand_f32(seed) * TAU_F;
+                        seed += 1u;
+                        float xi = rand_f32(seed);
+                        seed += 1u;
+                        float c0 = 1.0f, c1 = 0.0f;
+                        v3 dir_markov = splat(0.0f);
+                        if (GUIDE) {
+                            v3 ld = light_dir(s, ro);
+                            v3 mean = normalize(ld);
+                            float kappa = get_kappa(s);
+                            float W1 = logf(1.0f + (xi * exp_minus_one(-2.0f * kappa))) / kappa;
+                            float W = 1.0f + W1;
+                            float nV = sqrtf(-fmaf(W1, W1, 2.0f * W1));
+                            v3 Xs = from_onb_no_tangent(mk(strip_nan(cosf(theta) * nV), W, strip_nan(sinf(theta) * nV)), mean);
+                            dir_markov = normalize(Xs);
+                            float u0 = 0.2f, u1 = 0.8f;
+                            if (!(s.weight_sum > 0.0f) || near_zero(len(ld)) || near_zero(s.weight_sum) || near_zero(len(Xs))) {
+                                u0 = 1.0f;
+                                u1 = 0.0f;
+                            }
+                            float cs = u0 + u1;
+                            c0 = u0 / cs;
+                            c1 = u1 / cs;
+                        }
+                        float rnd = rand_f32(seed);
+                        seed += 1u;
+                        v3 dir;
+                        if (rnd < c0) {
+                            dir = dir_cos;
+                            last_not_vmf = true;
+                        } else {
+                            dir = dir_markov;
+                        }
+                        float mix_pdf = 0.0f;
+                        if (GUIDE && c1 != 0.0f && sum_mc > 0.0f) {
+                            for (int k = 0; k < NUM_RESAMPLES; ++k) {
+                                if (!(cand[k].weight_sum > 0.0f)) continue;
+                                mix_pdf += vmf_pdf(normalize(light_dir(cand[k], ro)), get_kappa(cand[k]), dir) *
+                                           (cand[k].weight_sum / sum_mc);
+                            }
+                        }
+                        float avg_pdf = (c0 * cos_pdf) + (c1 == 0.0f ? 0.0f : c1 * fmaxf(mix_pdf, 0.0f));
+                        v3 diffuse = Shader<Q, GUIDE>::make_diffuse(is.color, rd, is.normal, is.tangent, is.roughness.x, dir);
+                        cached_pdf = avg_pdf;
+                        cached_brdf = fmaxf(dot(dir, is.normal) / PI_F, 0.0f);
+                        float nf = fabsf(cached_brdf) / fmaxf(avg_pdf, 0.001f);
+                        color = (color * nf) * diffuse;
+                        orc = (orc * nf) * diffuse;
+                        rd = dir;
+                    } else if (is.ty == TY_TRANSPARENT) {
+                        cached_pdf = 1.0f;
+                        cached_brdf = 1.0f;
+                        rd = refract(rd, normal, ri);
+                    }
+                } else {
+                    cached_pdf = 1.0f;
+                    cached_brdf = 1.0f;
+                    rd = reflect(rd, normal);
+                    if (dot(rd, is.normal) < 0.0f) rd = reflect(rd, is.normal);
+                }
+                cont = depth + 1u < A.max_depth;
+                terminated = !cont;
+            } else {
+                v3 bg = sky_sample(A.S, rd);
+                v3 new_pos = fma3(rd, splat(A.tmax), ro);
+                if (depth == 1u && rec) {
+                    A.vpoint[path] = make_float4(new_pos.x, new_pos.y, new_pos.z, 0.0f);
+                    A.vnormal[path] = make_float4(-rd.x, -rd.y, -rd.z, 0.0f);
+                }
+                if (depth == 0u && last_sample) {
+                    if (A.out_normal) A.out_normal[pixel] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+                    if (A.out_albedo) A.out_albedo[pixel] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+                    if (A.pix_emission) {
+                        A.pix_emission[pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        A.pix_albedo[pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    }
+                }
+                if (depth != 0u) {
+                    orad = fma3(orc, bg, orad);
+                    v3 rad_out = (bg * cached_brdf) / cached_pdf;
+                    if (GUIDE) grid_add_radiance(G, ro, last_normal, last_dir, rad_out);
+                    float weight = len(rad_out);
+                    if (weight > 0.0f) {
+                        if (GUIDE) {
+                            MC st = update_chain(ro, new_pos, weight, seed, false, grid_load(G, ro, last_normal, last_dir, false),
+                                                 1.0f, sum_mc);
+                            grid_store(G, ro, last_normal, last_dir, st);
+                            tentative = update_chain(ro, new_pos, len(rad_out), seed, false, tentative,
+                                                     depth == 1u ? 1.0f : 0.5f, sum_mc);
+                        }
+                        seed++;
+                    }
+                }
+                scol = fma3(color, bg, scol);
+                terminated = true;
+            }
+            if (terminated && GUIDE) {
+                // final training at the primary vertex (general.wesl:942-948)
+                v3 spt = mk(pp.x, pp.y, pp.z), snm = mk(pn.x, pn.y, pn.z);
+                float4 vp = A.vpoint[path];
+                v3 start_dir;
+                {
+                    v3 o0;
+                    create_ray(A, pixel % A.width, pixel / A.width, &o0, &start_dir);
+                }
+                MC wc = grid_load(G, spt, snm, start_dir, false);
+                MC st = update_chain(spt, mk(vp.x, vp.y, vp.z), len(orad), seed, false, wc, 1.0f, sum_mc);
+                grid_store(G, spt, snm, start_dir, st);
+                grid_add_radiance(G, spt, snm, start_dir, orad);
+            }
+            // write back
+            A.acc[path] = make_float4(scol.x, scol.y, scol.z, cached_pdf);
+            if (cont) {
+                A.thr[path] = make_float4(color.x, color.y, color.z, picked);
+                A.brdf[path] = cached_brdf;
+                A.seed[path] = seed;
+                A.flags[path] = (depth + 1u) | (last_not_vmf ? 0x100u : 0u);
+                A.ray_o[path] = make_float4(ro.x, ro.y, ro.z, 0.0f);
+                A.ray_d[path] = make_float4(rd.x, rd.y, rd.z, 0.0f);
+            }
+            if (rec) {
+                A.ort[path] = make_float4(orc.x, orc.y, orc.z, sum_mc);
+                A.orad[path] = make_float4(orad.x, orad.y, orad.z, 0.0f);
+                A.ppoint[path] = pp;
+                A.pnormal[path] = pn;
+            }
+            if (GUIDE) {
+                A.lnormal[path] = make_float4(last_normal.x, last_normal.y, last_normal.z, 0.0f);
+                A.ldir[path] = make_float4(last_dir.x, last_dir.y, last_dir.z, 0.0f);
+                mc_store(A.tent_live + pixel, tentative);
+            }
+        }
+        // warp-aggregated append of the surviving paths
+        const uint32_t mask = __ballot_sync(0xFFFFFFFFu, cont);
+        if (mask) {
+            uint32_t slot = 0;
+            if (lane == 0) slot = atomicAdd(A.count_out, __popc(mask));
+            slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+            if (cont) A.q_out[slot + __popc(mask & ((1u << lane) - 1u))] = path;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- per-pixel accumulate / outputs
+LAM_DEV void reservoir_update(lam_reservoir& R, v3 vp, uint32_t vn, v3 sp, uint32_t sn, v3 orad, uint32_t ty,
+                              float rough, float w_new, uint32_t seed) {
+    R.w = R.w + w_new;
+    uint32_t c = (R.packed_confidence_valid & 0x7FFFFFFFu) + 1u;
+    R.packed_confidence_valid = (c & 0x7FFFFFFFu) | (R.packed_confidence_valid & 0x80000000u);
+    if (rand_f32(seed) * R.w < w_new) {
+        R.visible_point[0] = vp.x; R.visible_point[1] = vp.y; R.visible_point[2] = vp.z;
+        R.visible_normal = vn;
+        R.sample_point[0] = sp.x; R.sample_point[1] = sp.y; R.sample_point[2] = sp.z;
+        R.sample_normal = sn;
+        R.out_radiance[0] = orad.x; R.out_radiance[1] = orad.y; R.out_radiance[2] = orad.z;
+        R.ty = ty;
+        R.roughness = rough;
+        R.packed_confidence_valid |= 0x80000000u;
+    }
+}
+LAM_DEV float res_p_hat(const lam_reservoir& R) {
+    return fmaxf(len(mk(R.out_radiance[0], R.out_radiance[1], R.out_radiance[2])), 0.00001f);
+}
+
+template <int Q>
+__global__ void __launch_bounds__(WAVE_BLOCK) accumulate_kernel(Args A, uint32_t is_last_wave) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.npix) return;
+    float4 pc = A.pix_color[p];
+    v3 col = mk(pc.x, pc.y, pc.z);
+    v3 orsum = splat(0.0f);
+    if (A.pix_orad) {
+        float4 t = A.pix_orad[p];
+        orsum = mk(t.x, t.y, t.z);
+    }
+    for (uint32_t j = 0; j < A.wave_count; ++j) {
+        const uint32_t path = j * A.npix + p;
+        float4 a = A.acc[path];
+        col = col + mk(a.x, a.y, a.z);
+        if (A.pix_orad) {
+            float4 o = A.orad[path];
+            orsum = orsum + mk(o.x, o.y, o.z);
+        }
+        if (A.restir == LAM_RESTIR_PER_SAMPLE && A.reservoirs) {
+            float4 pp = A.ppoint[path], pn = A.pnormal[path], vp = A.vpoint[path], vn = A.vnormal[path], o = A.orad[path];
+            uint32_t ty = __float_as_uint(pp.w);
+            lam_reservoir R = A.reservoirs[p];
+            if (ty != TY_SKY) {
+                v3 orr = mk(o.x, o.y, o.z);
+                float w = fmaxf(len(orr), 0.00001f);
+                uint32_t st = A.pixel_seed[p];
+                reservoir_update(R, mk(vp.x, vp.y, vp.z), normalised_to_u32(mk(vn.x, vn.y, vn.z)), mk(pp.x, pp.y, pp.z),
+                                 normalised_to_u32(mk(pn.x, pn.y, pn.z)), orr, ty, 0.0f, w, st);
+                A.pixel_seed[p] = rand_u32(st);
+                uint32_t c = R.packed_confidence_valid & 0x7FFFFFFFu;
+                R.W = safe_div(R.w, __uint2float_rn(c) * res_p_hat(R));
+            } else {
+                R.ty = TY_SKY;
+            }
+            A.reservoirs[p] = R;
+        }
+    }
+    A.pix_color[p] = make_float4(col.x, col.y, col.z, 0.0f);
+    if (A.pix_orad) A.pix_orad[p] = make_float4(orsum.x, orsum.y, orsum.z, 0.0f);
+    if (!is_last_wave) return;
+    const float inv_n = __uint2float_rn(A.samples);
+    if (A.out_color) {
+        v3 c = col / inv_n;
+        A.out_color[p] = make_float4(fmaxf(c.x, 0.0f), fmaxf(c.y, 0.0f), fmaxf(c.z, 0.0f), 1.0f);
+    }
+    const uint32_t last_path = (A.wave_count - 1u) * A.npix + p;
+    if (A.restir != LAM_RESTIR_DISABLED && A.info) {
+        float4 e = A.pix_emission[p], al = A.pix_albedo[p];
+        lam_info inf;
+        inf.arr[0] = A.camera_pos.x; inf.arr[1] = A.camera_pos.y; inf.arr[2] = A.camera_pos.z;
+        inf.arr[3] = e.x; inf.arr[4] = e.y; inf.arr[5] = e.z;
+        inf.arr[6] = al.x; inf.arr[7] = al.y; inf.arr[8] = al.z;
+        A.info[p] = inf;
+    }
+    if (A.tent_snap && A.chains && p < A.chains_len) A.chains[p] = A.tent_snap[p];
+    if (A.reservoirs) {
+        if (A.restir == LAM_RESTIR_PER_PIXEL) {
+            float4 pp = A.ppoint[last_path], pn = A.pnormal[last_path], vp = A.vpoint[last_path], vn = A.vnormal[last_path];
+            uint32_t ty = __float_as_uint(pp.w);
+            lam_reservoir R = lam_reservoir{};
+            if (ty != TY_SKY) {
+                v3 orr = orsum / inv_n;
+                float w = fmaxf(len(orr), 0.00001f);
+                uint32_t st = A.pixel_seed[p];
+                reservoir_update(R, mk(vp.x, vp.y, vp.z), normalised_to_u32(mk(vn.x, vn.y, vn.z)), mk(pp.x, pp.y, pp.z),
+                                 normalised_to_u32(mk(pn.x, pn.y, pn.z)), orr, ty, 0.0f, w, st);
+                uint32_t c = R.packed_confidence_valid & 0x7FFFFFFFu;
+                R.W = safe_div(R.w, __uint2float_rn(c) * res_p_hat(R));
+            } else {
+                R.ty = TY_SKY;
+            }
+            A.reservoirs[p] = R;
+        } else if (A.restir == LAM_RESTIR_DISABLED) {
+            A.reservoirs[p] = lam_reservoir{};
+        }
+    }
+}
+
+// subgroupShuffle(tentative, (lane + 1) % 32) after each sample (general.wesl:349-361, 582)
+__global__ void shuffle_kernel(Args A) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.npix) return;
+    const uint32_t x = p % A.width, y = p / A.width;
+    const uint32_t src_x = (x & ~31u) + (((x & 31u) + 1u) & 31u);
+    MC t = src_x < A.width ? mc_load(A.tent_live + (uint64_t)y * A.width + src_x) : mc_zero();
+    mc_store(A.tent_snap + p, t);
+}
+
+static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool full, bool guide) {
+    const uint32_t npix = width * height;
+    uint32_t spp_wave = 1;
+    if (!guide && pl->opts.restir_temporal != LAM_RESTIR_PER_SAMPLE) {
+        // enough paths in flight to fill the GPU: aim for ~8M paths, at most the sample count
+        uint64_t target = 8ull << 20;
+        spp_wave = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(pl->opts.samples, target / std::max(1u, npix)));
+    }
+    WaveBuffers* w = pl->wave;
+    if (w && w->width == width && w->height == height && w->spp_wave == spp_wave && w->full == full && w->guide == guide)
+        return LAM_OK;
+    free_wave(w);
+    pl->wave = nullptr;
+    w = new WaveBuffers();
+    w->width = width;
+    w->height = height;
+    w->npix = npix;
+    w->spp_wave = spp_wave;
+    w->paths = (uint64_t)npix * spp_wave;
+    w->full = full;
+    w->guide = guide;
+    const size_t P = w->paths;
+    int rc = 0;
+    rc |= walloc(w, &w->ray_o, P);
+    rc |= walloc(w, &w->ray_d, P);
+    rc |= walloc(w, &w->hit, P);
+    rc |= walloc(w, &w->queue0, P);
+    rc |= walloc(w, &w->queue1, P);
+    rc |= walloc(w, &w->thr, P);
+    rc |= walloc(w, &w->acc, P);
+    rc |= walloc(w, &w->brdf, P);
+    rc |= walloc(w, &w->seed, P);
+    rc |= walloc(w, &w->flags, P);
+    rc |= walloc(w, &w->pix_color, npix);
+    rc |= walloc(w, &w->ctr, 64);
+    if (full) {
+        rc |= walloc(w, &w->ort, P);
+        rc |= walloc(w, &w->orad, P);
+        rc |= walloc(w, &w->ppoint, P);
+        rc |= walloc(w, &w->pnormal, P);
+        rc |= walloc(w, &w->vpoint, P);
+        rc |= walloc(w, &w->vnormal, P);
+        rc |= walloc(w, &w->pix_orad, npix);
+        rc |= walloc(w, &w->pix_emission, npix);
+        rc |= walloc(w, &w->pix_albedo, npix);
+    }
+    if (guide) {
+        rc |= walloc(w, &w->lnormal, P);
+        rc |= walloc(w, &w->ldir, P);
+        rc |= walloc(w, &w->tent_snap, npix);
+        rc |= walloc(w, &w->tent_live, npix);
+    }
+    if (rc) {
+        free_wave(w);
+        return LAM_ERR_CUDA;
+    }
+    cudaMemset(w->ctr, 0, 64 * sizeof(uint32_t));
+    pl->total_segments = 0;
+    pl->prof_segments_base = 0;
+    cudaDeviceGetAttribute(&w->sms, cudaDevAttrMultiProcessorCount, pl->device);
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, extend_kernel<false>, WAVE_BLOCK, 0);
+    w->grid_extend = w->sms * std::max(1, occ);
+    occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_kernel<LAM_QUALITY_MEDIUM, false>, WAVE_BLOCK, 0);
+    w->grid_shade = w->sms * std::max(1, occ);
+    pl->wave = w;
+    return LAM_OK;
+}
+
+template <int Q>
+static void launch_shade(bool guide, dim3 g, dim3 b, cudaStream_t st, const Args& A) {
+    if (guide) shade_kernel<Q, true><<<g, b, 0, st>>>(A);
+    else shade_kernel<Q, false><<<g, b, 0, st>>>(A);
+}
+
+}  // namespace lam
+
+using namespace lam;
+
+extern "C" int lam_tracer_create_pipeline(const lam_tracer* t, const lam_pipeline_layout* layout,
+                                          const lam_tracer_options* o, lam_pipeline** out) {
+    if (!t || !layout || !o || !out) return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_tracer_create_pipeline: null argument");
+    if (o->samples == 0) return set_error(LAM_ERR_INVALID_ARGUMENT, "samples must be nonzero (NonZeroU32)");
+    if (o->max_depth == 0 || o->max_depth > 255) return set_error(LAM_ERR_INVALID_ARGUMENT, "max_depth must be in 1..255");
+    if (o->restir_temporal > LAM_RESTIR_PER_PIXEL) return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown ReSTIR mode");
+    if (o->guide_mode > LAM_GUIDE_LEARNED) return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown guide mode");
+    if (o->guide_mode == LAM_GUIDE_LEARNED) return set_error(LAM_ERR_UNSUPPORTED, "learned guiding is not available in this pipeline");
+    if (t->quality > LAM_QUALITY_HIGH) return set_error(LAM_ERR_UNSUPPORTED, "debug shaders are rendered with lam_render_debug");
+    lam_pipeline* p = new lam_pipeline();
+    p->quality = t->quality;
+    p->opts = *o;
+    p->layout = *layout;
+    p->intersection_handler = t->intersection_handler;
+    cudaGetDevice(&p->device);
+    *out = p;
+    return LAM_OK;
+}
+
+extern "C" int lam_pipeline_destroy(lam_pipeline* p) {
+    if (!p) return LAM_OK;
+    free_wave(p->wave);
+    for (auto& t : p->timed) {
+        cudaEventDestroy(t.start);
+        cudaEventDestroy(t.end);
+    }
+    for (cudaEvent_t e : p->event_pool) cudaEventDestroy(e);
+    delete p;
+    return LAM_OK;
+}
+
+extern "C" int lam_pipeline_set_profiling(lam_pipeline* p, int enabled) {
+    if (!p) return set_error(LAM_ERR_INVALID_ARGUMENT, "null pipeline");
+    p->profiling = enabled != 0;
+    return LAM_OK;
+}
+
+extern "C" int lam_render_profile_get(lam_pipeline* p, lam_stage_times* out) {
+    if (!p || !out) return set_error(LAM_ERR_INVALID_ARGUMENT, "null argument");
+    for (auto& t : p->timed) {
+        cudaError_t e = cudaEventSynchronize(t.end);
+        if (e != cudaSuccess) return cuda_error(e, "lam_render_profile_get");
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, t.start, t.end);
+        switch (t.stage) {
+            case 0: p->prof.generate_ms += ms; break;
+            case 1: p->prof.extend_ms += ms; p->prof.extend_launches++; break;
+            case 2: p->prof.shade_ms += ms; p->prof.shade_launches++; break;
+            default: p->prof.accumulate_ms += ms; break;
+        }
+        p->event_pool.push_back(t.start);
+        p->event_pool.push_back(t.end);
+    }
+    p->timed.clear();
+    lam_render_stats s;
+    p->stats_pending = true;
+    int rc = lam_render_stats_get(p, &s);
+    if (rc) return rc;
+    *out = p->prof;
+    out->ray_segments = p->total_segments - p->prof_segments_base;
+    return LAM_OK;
+}
+
+extern "C" int lam_render_profile_reset(lam_pipeline* p) {
+    if (!p) return set_error(LAM_ERR_INVALID_ARGUMENT, "null pipeline");
+    lam_stage_times tmp;
+    int rc = lam_render_profile_get(p, &tmp);
+    if (rc) return rc;
+    p->prof = lam_stage_times{};
+    p->prof_segments_base = p->total_segments;
+    return LAM_OK;
+}
+
+// Reads the device counters of the last render (synchronises the device).
+extern "C" int lam_render_stats_get(const lam_pipeline* p, lam_render_stats* out) {
+    if (!p || !out) return set_error(LAM_ERR_INVALID_ARGUMENT, "null argument");
+    lam_pipeline* q = const_cast<lam_pipeline*>(p);
+    if (q->stats_pending && q->wave) {
+        uint32_t host[16];
+        cudaError_t e = cudaMemcpy(host, q->wave->ctr, sizeof(host), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_error(e, "lam_render_stats_get");
+        unsigned long long segs, total;
+        std::memcpy(&segs, host + 8, sizeof(segs));
+        std::memcpy(&total, host + 10, sizeof(total));
+        q->stats.ray_segments = segs;
+        q->total_segments = total;
+        q->stats.error_flags = host[4];
+        q->stats_pending = false;
+    }
+    *out = q->stats;
+    return LAM_OK;
+}
+
+extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers* b, const lam_camera* cam,
+                          const lam_frame_targets* tg, uint32_t seed_offset, void* stream) {
+    if (!pl || !s || !b || !cam || !tg) return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_render: null argument");
+    if (tg->width == 0 || tg->height == 0) return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_render: empty target");
+    if (tg->width != b->width || tg->height != b->height)
+        return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_render: targets and data buffers differ in size");
+    if ((uint64_t)tg->width * tg->height > 0xFFFFFFFFull / 4)
+        return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_render: target too large");
+    if (s->instance_count > pl->layout.blas_count || s->diffuse_count > pl->layout.diffuse_count ||
+        s->emission_count > pl->layout.emission_count || s->attribute_count > pl->layout.attribute_count)
+        return set_error(LAM_ERR_LAYOUT_MISMATCH, "scene bindings exceed the pipeline layout counts");
+    const bool guide = pl->opts.guide_mode == LAM_GUIDE_MARKOV;
+    const uint32_t restir = pl->opts.restir_temporal;
+    const bool full = guide || restir != LAM_RESTIR_DISABLED;
+    int rc = ensure_wave(pl, tg->width, tg->height, full, guide);
+    if (rc) return rc;
+    WaveBuffers* w = pl->wave;
+    cudaStream_t st = (cudaStream_t)stream;
+    Args A;
+    std::memset(&A, 0, sizeof(A));
+    A.S = s->dev;
+    A.cam = *cam;
+    A.width = tg->width;
+    A.height = tg->height;
+    A.npix = w->npix;
+    A.samples = pl->opts.samples;
+    A.max_depth = pl->opts.max_depth;
+    A.restir = restir;
+    A.seed_offset = seed_offset;
+    A.tmin = pl->opts.tmin;
+    A.tmax = pl->opts.tmax;
+    A.ray_o = w->ray_o;
+    A.ray_d = w->ray_d;
+    A.hit = w->hit;
+    A.err = w->ctr + 4;
+    A.segments = reinterpret_cast<unsigned long long*>(w->ctr + 8);
+    A.thr = w->thr;
+    A.acc = w->acc;
+    A.brdf = w->brdf;
+    A.seed = w->seed;
+    A.flags = w->flags;
+    A.ort = w->ort;
+    A.orad = w->orad;
+    A.ppoint = w->ppoint;
+    A.pnormal = w->pnormal;
+    A.vpoint = w->vpoint;
+    A.vnormal = w->vnormal;
+    A.lnormal = w->lnormal;
+    A.ldir = w->ldir;
+    A.pix_color = w->pix_color;
+    A.pix_orad = w->pix_orad;
+    A.pix_emission = w->pix_emission;
+    A.pix_albedo = w->pix_albedo;
+    A.tent_snap = w->tent_snap;
+    A.tent_live = w->tent_live;
+    const bool screen = (b->types & LAM_BUFFER_MARKOV_CHAIN_SCREEN_SPACE) != 0u;
+    const bool world = (b->types & LAM_BUFFER_MARKOV_CHAIN_WORLD_SPACE) != 0u;
+    A.old_chains = guide && screen ? (const lam_markov_chain*)b->old_chains : nullptr;
+    A.old_chains_len = b->chain_len;
+    A.chains = guide && screen ? (lam_markov_chain*)b->chains : nullptr;
+    A.chains_len = b->chain_len;
+    A.world = (uint32_t*)b->world;
+    A.old_world = (const uint32_t*)b->old_world;
+    A.world_len = b->world_len;
+    A.reservoirs = (lam_reservoir*)b->reservoirs;
+    if (b->reservoir_len < w->npix) A.reservoirs = nullptr;
+    A.info = (lam_info*)b->info;
+    A.pixel_seed = (uint32_t*)b->pixel_seed;
+    A.out_color = (float4*)tg->color;
+    A.out_normal = (float4*)tg->normal;
+    A.out_albedo = (float4*)tg->albedo;
+    A.camera_pos = v3{cam->view_inverse[12], cam->view_inverse[13], cam->view_inverse[14]};
+    if (guide && !world) return set_error(LAM_ERR_INVALID_ARGUMENT, "Markov guiding needs MARKOV_CHAIN_WORLD_SPACE buffers");
+    const bool alpha = !s->dev.all_opaque;
+    const dim3 blk(WAVE_BLOCK);
+    const dim3 gpix((w->npix + WAVE_BLOCK - 1) / WAVE_BLOCK);
+    uint32_t launches = 0;
+    auto ev = [&]() {
+        cudaEvent_t e;
+        if (!pl->event_pool.empty()) {
+            e = pl->event_pool.back();
+            pl->event_pool.pop_back();
+        } else {
+            cudaEventCreate(&e);
+        }
+        return e;
+    };
+    // stage 0 generate, 1 extend, 2 shade, 3 accumulate/shuffle
+    auto begin = [&](int stage) -> int {
+        if (!pl->profiling) return -1;
+        lam_pipeline::Timed t{stage, ev(), ev()};
+        cudaEventRecord(t.start, st);
+        pl->timed.push_back(t);
+        return (int)pl->timed.size() - 1;
+    };
+    auto end = [&](int h) {
+        if (h >= 0) cudaEventRecord(pl->timed[h].end, st);
+    };
+    cudaMemsetAsync(w->ctr, 0, 10 * sizeof(uint32_t), st);  // keeps the cumulative counter ctr[10..11]
+    for (uint32_t first = 0; first < pl->opts.samples; first += w->spp_wave) {
+        A.wave_first = first;
+        A.wave_count = std::min(w->spp_wave, pl->opts.samples - first);
+        uint32_t* qa = w->queue0;
+        uint32_t* qb = w->queue1;
+        uint32_t* ca = w->ctr + 0;
+        uint32_t* cb = w->ctr + 1;
+        A.q_in = qa;
+        A.count_in = ca;
+        int h = begin(0);
+        generate_kernel<<<gpix, blk, 0, st>>>(A);
+        end(h);
+        ++launches;
+        for (uint32_t depth = 0; depth < pl->opts.max_depth; ++depth) {
+            A.q_in = qa;
+            A.q_out = qb;
+            A.count_in = ca;
+            A.count_out = cb;
+            A.work = w->ctr + 2;
+            cudaMemsetAsync(w->ctr + 2, 0, sizeof(uint32_t), st);
+            cudaMemsetAsync(cb, 0, sizeof(uint32_t), st);
+            h = begin(1);
+            if (alpha) extend_kernel<true><<<w->grid_extend, blk, 0, st>>>(A);
+            else extend_kernel<false><<<w->grid_extend, blk, 0, st>>>(A);
+            end(h);
+            h = begin(2);
+            switch (pl->quality) {
+                case LAM_QUALITY_LOW: launch_shade<LAM_QUALITY_LOW>(guide, w->grid_shade, blk, st, A); break;
+                case LAM_QUALITY_HIGH: launch_shade<LAM_QUALITY_HIGH>(guide, w->grid_shade, blk, st, A); break;
+                default: launch_shade<LAM_QUALITY_MEDIUM>(guide, w->grid_shade, blk, st, A); break;
+            }
+            end(h);
+            launches += 2;
+            std::swap(qa, qb);
+            std::swap(ca, cb);
+        }
+        h = begin(3);
+        if (guide) {
+            shuffle_kernel<<<gpix, blk, 0, st>>>(A);
+            ++launches;
+        }
+        const uint32_t last = first + A.wave_count >= pl->opts.samples ? 1u : 0u;
+        accumulate_kernel<0><<<gpix, blk, 0, st>>>(A, last);
+        end(h);
+        ++launches;
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_error(e, "lam_render launch");
+    pl->stats.samples = (uint64_t)w->npix * pl->opts.samples;
+    pl->stats.kernel_launches = launches;
+    pl->stats_pending = true;
+    return LAM_OK;
+}

@@ -1,0 +1,108 @@
+"""Rendering parity: the wavefront path tracer against the oracle's restatement of rt_main."""
+import numpy as np
+import pytest
+
+import lambent_b200 as lb
+from lambent_b200 import _abi, scenes
+from oracle import oracle_py as O
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_render(s, samples, quality=_abi.QUALITY_MEDIUM, restir=_abi.RESTIR_PER_PIXEL, depth=5,
+               guide=_abi.GUIDE_NONE, seed=0, buffers=None, world=1 << 16):
+    import torch
+    tracer = lb.RayTracer(lb.api._Quality(quality, "q"))
+    opts = lb.PathTracerOpts(samples=samples, restir_temporal=restir, max_depth=depth, guide_mode=guide)
+    pipe = tracer.create_pipeline(*s.layout_counts(), opts)
+    g = lb.GpuScene(s)
+    W, H = s.width, s.height
+    bufs = buffers or lb.DataBuffers(W, H, world, _abi.BUFFER_ALL)
+    col, nrm, alb = (torch.zeros((H, W, 4), dtype=torch.float32, device="cuda") for _ in range(3))
+    tg = lb.targets_from(col, nrm, alb)
+    pipe.render(g, bufs, s.camera, tg, seed)
+    torch.cuda.synchronize()
+    st = pipe.stats()
+    return {"color": col.cpu().numpy(), "normal": nrm.cpu().numpy(), "albedo": alb.cpu().numpy(), "stats": st,
+            "buffers": bufs, "pipe": pipe, "scene": g}
+
+
+def read_buffer(bufs, which, dtype, shape):
+    import torch
+    ptr, n = bufs.device_buffer(which)
+    host = np.empty(n, np.uint8)
+    import ctypes
+    torch.cuda.synchronize()
+    ctypes.CDLL("libcudart.so").cudaMemcpy(host.ctypes.data_as(ctypes.c_void_p), ctypes.c_void_p(ptr),
+                                           ctypes.c_size_t(n), 2)
+    return host.view(dtype).reshape(shape)
+
+
+@pytest.mark.parametrize("quality", [_abi.QUALITY_LOW, _abi.QUALITY_MEDIUM, _abi.QUALITY_HIGH])
+def test_same_seed_matches_oracle(cuda, quality):
+    """Same seeds: both follow identical random streams, so pixels agree except where last-bit
+    differences in transcendental functions flip a branch."""
+    s = scenes.cornell_box(64, 64)
+    spp = 8
+    g = gpu_render(s, spp, quality=quality, restir=_abi.RESTIR_PER_PIXEL)
+    o = O.OracleScene(s).render(s.camera, 64, 64, samples=spp, quality=quality, restir=_abi.RESTIR_PER_PIXEL)
+    diff = np.abs(g["color"] - o["color"])[..., :3].max(-1)
+    close = diff <= 1e-3 * np.maximum(1.0, np.abs(o["color"][..., :3]).max(-1))
+    assert close.mean() > 0.97, close.mean()
+    np.testing.assert_allclose(g["normal"], o["normal"], atol=1e-5)
+    np.testing.assert_allclose(g["albedo"], o["albedo"], atol=1e-6)
+    assert g["stats"].samples == 64 * 64 * spp
+    # ray segments agree within the few diverged paths
+    assert abs(g["stats"].ray_segments - o["segments"]) <= 0.03 * o["segments"]
+
+
+def test_reservoirs_and_info_match_oracle(cuda):
+    s = scenes.cornell_box(64, 64)
+    g = gpu_render(s, 4, restir=_abi.RESTIR_PER_PIXEL)
+    o = O.OracleScene(s).render(s.camera, 64, 64, samples=4, restir=_abi.RESTIR_PER_PIXEL)
+    P = 64 * 64
+    gi = read_buffer(g["buffers"], lb.DataBuffers.INFO, np.float32, (P, 9))
+    np.testing.assert_allclose(gi, o["buffers"]["info"], atol=1e-5)
+    gr = read_buffer(g["buffers"], lb.DataBuffers.RESERVOIRS, np.float32, (P, 16))
+    orr = o["buffers"]["reservoirs"]
+    same = np.all(np.isclose(gr, orr, rtol=1e-3, atol=1e-4), axis=1)
+    assert same.mean() > 0.95
+
+
+def test_statistical_agreement_independent_seeds(cuda):
+    """Different seeds: per-pixel means agree within 3 sigma of the combined sample variance."""
+    s = scenes.cornell_box(32, 32)
+    spp, reps = 64, 6
+    gs = np.stack([gpu_render(s, spp, restir=_abi.RESTIR_DISABLED, seed=1000 + r)["color"][..., :3] for r in range(reps)])
+    osc = O.OracleScene(s)
+    os_ = np.stack([osc.render(s.camera, 32, 32, samples=spp, restir=_abi.RESTIR_DISABLED, seed_offset=5000 + r)["color"][..., :3]
+                    for r in range(reps)])
+    gm, om = gs.mean(0), os_.mean(0)
+    var = gs.var(0, ddof=1) / reps + os_.var(0, ddof=1) / reps
+    z = np.abs(gm - om) / np.sqrt(var + 1e-12)
+    ok = (z <= 3.0) | (np.abs(gm - om) < 1e-6)
+    assert ok.mean() > 0.97, ok.mean()
+    assert abs(gm.mean() - om.mean()) < 0.02 * om.mean() + 1e-3
+
+
+def test_markov_guiding_is_unbiased(cuda):
+    """Guided (Markov chains) and unguided renders converge to the same image."""
+    s = scenes.cornell_box(32, 32)
+    plain = np.stack([gpu_render(s, 64, restir=_abi.RESTIR_DISABLED, seed=r)["color"][..., :3] for r in range(4)]).mean(0)
+    guided = np.stack([gpu_render(s, 64, restir=_abi.RESTIR_DISABLED, guide=_abi.GUIDE_MARKOV, seed=100 + r)["color"][..., :3]
+                       for r in range(4)]).mean(0)
+    assert np.isfinite(guided).all()
+    assert abs(guided.mean() - plain.mean()) < 0.08 * plain.mean()
+
+
+def test_depth_and_layout_errors(cuda):
+    s = scenes.cornell_box(16, 16)
+    t = lb.RayTracer(lb.path_tracing.Medium)
+    with pytest.raises(lb.LambentError):
+        t.create_pipeline(1, 4, 1, 1, lb.PathTracerOpts(samples=1, max_depth=0))
+    pipe = t.create_pipeline(1, 1, 1, 1, lb.PathTracerOpts(samples=1))
+    import torch
+    col = torch.zeros((16, 16, 4), dtype=torch.float32, device="cuda")
+    with pytest.raises(lb.LambentError) as e:
+        pipe.render(lb.GpuScene(s), lb.DataBuffers(16, 16, 16, 7), s.camera, lb.targets_from(col))
+    assert e.value.code == _abi.ERR_LAYOUT_MISMATCH

@@ -1,0 +1,103 @@
+"""The CPU oracle, pinned against the known-answer vectors (tests/golden/kat.json) and checked
+against itself (BVH traversal vs brute force, determinism)."""
+import ctypes as C
+import json
+import os
+
+import numpy as np
+
+from lambent_b200 import scenes, _abi
+from oracle import oracle_py as O
+
+KAT = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "kat.json")))
+
+
+def test_rng_known_answers():
+    L = O.lib()
+    for s, v in KAT["rand_u32"]:
+        assert L.oracle_rand_u32(s) == v
+    for s, v in KAT["rand_f32"]:
+        assert np.float32(L.oracle_rand_f32(s)) == np.float32(v)
+
+
+def test_half_and_bfloat_known_answers():
+    L = O.lib()
+    for f, bits in KAT["f16"]:
+        assert L.oracle_f32_to_f16(f) == bits, f
+    for f, bits in KAT["bf16"]:
+        assert L.oracle_f32_to_bf16(f) == bits, f
+    for f, bits in KAT["f16"]:
+        if bits & 0x7C00 != 0x7C00:
+            back = L.oracle_f16_to_f32(bits)
+            assert back == float(np.uint16(bits).view(np.float16))
+
+
+def test_octahedral_known_answers_and_round_trip():
+    L = O.lib()
+    for n, code in KAT["octahedral"]:
+        assert L.oracle_normalised_to_u32((C.c_float * 3)(*n)) == code, n
+        out = (C.c_float * 3)()
+        L.oracle_u32_to_normalised(code, out)
+        assert np.dot(np.array(out[:]), np.array(n)) > 0.9998
+
+
+def random_rays(n, rng, lo, hi):
+    o = rng.uniform(lo, hi, (n, 3))
+    d = rng.normal(size=(n, 3))
+    r = np.zeros((n, 8), np.float32)
+    r[:, 0:3], r[:, 3], r[:, 4:7], r[:, 7] = o, 1e-4, d, 1000.0
+    return r
+
+
+def small_field(seed=3):
+    return scenes.icosphere_field(64, 64, instances=6, subdiv=3, tex_size=16, tex_layers=2, seed=seed)
+
+
+def test_oracle_bvh_matches_bruteforce():
+    rng = np.random.default_rng(0)
+    for s, lo, hi in ((scenes.cornell_box(16, 16), -0.99, 1.9), (small_field(), -12.0, 12.0)):
+        osc = O.OracleScene(s)
+        rays = random_rays(20000, rng, lo, hi)
+        a = osc.trace(rays)
+        b = osc.trace(rays, bruteforce=True)
+        np.testing.assert_array_equal(a, b)
+
+
+def test_watertight_closed_mesh():
+    # every ray from inside a closed icosphere must hit it (no cracks along shared edges / vertices)
+    s = scenes.Scene()
+    v, f = scenes.icosphere(4)
+    s.blas.append({"vertices": v.astype(np.float32), "indices": f.astype(np.uint32).reshape(-1), "flags": 1})
+    s.instances.append({"transform": scenes.IDENTITY.copy(), "blas": 0, "material_indices": np.zeros(f.shape[0], np.uint32)})
+    osc = O.OracleScene(s)
+    rng = np.random.default_rng(5)
+    n = 20000
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 4:7] = v[rng.integers(0, v.shape[0], n)] + rng.normal(0, 1e-7, (n, 3))  # aim at vertices / edges
+    rays[:, 3], rays[:, 7] = 0.0, 10.0
+    h = osc.trace(rays)
+    assert (h["kind"] != 0).all()
+
+
+def test_oracle_render_deterministic_single_thread():
+    s = scenes.cornell_box(32, 32)
+    osc = O.OracleScene(s)
+    a = osc.render(s.camera, 32, 32, samples=4, threads=1, guide=_abi.GUIDE_MARKOV)
+    b = osc.render(s.camera, 32, 32, samples=4, threads=1, guide=_abi.GUIDE_MARKOV)
+    np.testing.assert_array_equal(a["color"], b["color"])
+    assert a["segments"] >= 32 * 32 * 4
+    assert a["samples"] == 32 * 32 * 4
+
+
+def test_oracle_resampling_passes_run():
+    s = scenes.cornell_box(32, 32)
+    osc = O.OracleScene(s)
+    r = osc.render(s.camera, 32, 32, samples=4, threads=1)
+    b = r["buffers"]
+    res = b["reservoirs"].copy()
+    O.temporal(res, b["old_reservoirs"], 32, 32, 0)
+    out = O.spatial(res, b["info"], 32, 32, 5, 61, 0)
+    assert np.isfinite(out).all()
+    O.process_gi(res, 20)
+    conf = res.view(np.uint32)[:, 14] & 0x7FFFFFFF
+    assert conf.max() <= 20
