@@ -325,19 +325,19 @@ __global__ void __launch_bounds__(TRACE_BLOCK) trace_rays_kernel(DevScene S, con
     const uint4* tl;
     const DevInstance* in;
     stage_tlas(S, sm, tl, in);
-    const uint32_t lane = threadIdx.x & 31u;
     uint32_t err = 0u;
-    for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(counter, 32u);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= n) break;
-        const uint32_t i = base + lane;
-        if (i >= n) continue;
+    auto load = [&](uint32_t i, float3& o, float3& d, float& t0, float& t1) {
+        const float4 r0 = __ldg(reinterpret_cast<const float4*>(rays + i));
+        const float4 r1 = __ldg(reinterpret_cast<const float4*>(rays + i) + 1);
+        o = make_float3(r0.x, r0.y, r0.z);
+        d = make_float3(r1.x, r1.y, r1.z);
+        t0 = r0.w;
+        t1 = r1.w;
+    };
+    auto store = [&](uint32_t i, const TraceResult& tr) {
         const float4 r0 = __ldg(reinterpret_cast<const float4*>(rays + i));
         const float4 r1 = __ldg(reinterpret_cast<const float4*>(rays + i) + 1);
         const float3 o = make_float3(r0.x, r0.y, r0.z), d = make_float3(r1.x, r1.y, r1.z);
-        TraceResult tr = trace_ray<ANY, ALPHA>(S, tl, in, o, d, r0.w, r1.w, err);
         lam_hit h;
         if (tr.tri == NO_HIT) {
             h.t = 0.0f; h.u = 0.0f; h.v = 0.0f;
@@ -357,7 +357,8 @@ __global__ void __launch_bounds__(TRACE_BLOCK) trace_rays_kernel(DevScene S, con
             h.kind = front ? LAM_HIT_FRONT : LAM_HIT_BACK;
         }
         hits[i] = h;
-    }
+    };
+    trace_persistent<ANY, ALPHA>(S, tl, in, n, counter, err, load, store);
     if (err) atomicOr(err_out, err);
 }
 

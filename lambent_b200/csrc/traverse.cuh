@@ -209,6 +209,168 @@ struct TraceResult {
 // alpha is near zero, transparent materials always accepted (general.wesl:1059-1067).
 LAM_DEV bool alpha_accept(const DevScene& S, uint32_t inst, uint32_t prim, float bu, float bv);
 
+// Resumable traversal: init() then step() until it returns false.  One step intersects one node
+// and tests the leaf items it exposes, so a warp can refill lanes whose rays have finished
+// (after Aila and Laine, "Understanding the Efficiency of Ray Traversal on GPUs", HPG 2009).
+template <bool ANY, bool ALPHA>
+struct Traverser {
+    TravRay R;
+    float3 wo, wd;
+    float tmin, best_t;
+    uint2 ng, tg;
+    int sp, blas_base;
+    uint32_t cur_inst, cur_flags;
+    TraceResult res;
+
+    LAM_DEV void init(const DevScene& S, float3 o, float3 d, float t0, float t1) {
+        wo = o;
+        wd = d;
+        tmin = t0;
+        best_t = t1;
+        res.tri = NO_HIT;
+        res.inst = NO_HIT;
+        res.prim = NO_HIT;
+        res.t = t1;
+        sp = 0;
+        blas_base = -1;
+        cur_inst = 0u;
+        cur_flags = 0u;
+        setup_ray(R, o, d);
+        ng = S.tlas_node_count ? make_uint2(0u, (1u << (24u + R.oct)) | 1u) : make_uint2(0u, 0u);
+        tg = make_uint2(0u, 0u);
+    }
+
+    LAM_DEV void push(uint2* stack, uint2 g, uint32_t& err) {
+        if (sp < TRAVERSAL_STACK) stack[sp++] = g;
+        else err |= ERR_STACK_OVERFLOW;
+    }
+
+    // Returns false once the traversal has finished (res is final).  `stack` holds
+    // TRAVERSAL_STACK entries owned by this lane (kept outside the struct so that the struct
+    // itself stays in registers).
+    LAM_DEV bool step(const DevScene& S, const uint4* __restrict__ tlas_nodes, const DevInstance* __restrict__ insts,
+                      uint2* stack, uint32_t& err) {
+        if (ng.y > 0x00FFFFFFu) {
+            const uint32_t k = __ffs(ng.y >> 24) - 1u;
+            ng.y &= ~(1u << (24u + k));
+            const uint32_t slot = k ^ R.oct;
+            const uint32_t child = ng.x + __popc(ng.y & ((1u << slot) - 1u) & 0xFFu);
+            if (ng.y > 0x00FFFFFFu) push(stack, ng, err);
+            const uint4* nodes = blas_base < 0 ? tlas_nodes : S.blas_nodes;
+            intersect_node(nodes + 5u * child, R, tmin, best_t, ng, tg);
+        } else {
+            tg = ng;
+            ng = make_uint2(0u, 0u);
+        }
+        while (tg.y != 0u) {
+            const uint32_t k = __ffs(tg.y) - 1u;
+            tg.y &= tg.y - 1u;
+            const uint32_t item = tg.x + k;
+            if (blas_base < 0) {
+                const uint32_t id = __ldg(S.tlas_items + item);
+                const DevInstance& I = insts[id];
+                const uint32_t flags = I.flags;
+                const uint32_t root = I.blas_root;
+                if (!(flags & INST_VISIBLE) || root == NO_HIT) continue;
+                if (tg.y != 0u) push(stack, tg, err);
+                if (ng.y > 0x00FFFFFFu) push(stack, ng, err);
+                blas_base = sp;
+                cur_inst = id;
+                cur_flags = flags;
+                float m[12];
+#pragma unroll
+                for (int q = 0; q < 12; ++q) m[q] = I.inv[q];
+                float3 oo, od;
+                object_ray(m, wo, wd, &oo, &od);
+                setup_ray(R, oo, od);
+                ng = make_uint2(root, (1u << (24u + R.oct)) | 1u);
+                tg = make_uint2(0u, 0u);
+                return true;
+            }
+            const float4* tp = S.tris + 3u * item;
+            const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+            float t;
+            if (!wbw_f32(R, a, b, c, best_t, &t)) continue;
+            const uint32_t prim = __float_as_uint(a.w);
+            bool better = t > tmin && (t < best_t || (t == best_t && res.tri != NO_HIT &&
+                                                      (cur_inst < res.inst || (cur_inst == res.inst && prim < res.prim))));
+            if (!better) continue;
+            if (ALPHA && !(cur_flags & INST_OPAQUE)) {
+                float rt, ru, rv;
+                bool fr;
+                wbw_f64(R.o, R.d, a, b, c, &rt, &ru, &rv, &fr);
+                if (!alpha_accept(S, cur_inst, prim, ru, rv)) continue;
+            }
+            best_t = t;
+            res.tri = item;
+            res.inst = cur_inst;
+            res.prim = prim;
+            if (ANY) {
+                res.t = best_t;
+                return false;
+            }
+        }
+        if (ng.y <= 0x00FFFFFFu) {
+            if (blas_base >= 0 && sp == blas_base) {
+                blas_base = -1;
+                setup_ray(R, wo, wd);
+            }
+            if (sp == 0) {
+                res.t = best_t;
+                return false;
+            }
+            ng = stack[--sp];
+        }
+        return true;
+    }
+};
+
+// Lanes below this many active rays trigger a refill of the idle lanes from the work queue.
+#ifndef LAM_REFILL_THRESHOLD
+#define LAM_REFILL_THRESHOLD 20
+#endif
+constexpr int REFILL_THRESHOLD = LAM_REFILL_THRESHOLD;
+
+// Persistent warp loop over work items [0, n) claimed with a global counter.  `load(i, o, d, t0, t1)`
+// fetches item i; `store(i, res)` consumes a finished traversal.  Every lane of the warp must call it.
+template <bool ANY, bool ALPHA, class Load, class Store>
+LAM_DEV void trace_persistent(const DevScene& S, const uint4* __restrict__ tl, const DevInstance* __restrict__ in,
+                              uint32_t n, uint32_t* __restrict__ work, uint32_t& err, Load load, Store store) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    Traverser<ANY, ALPHA> T;
+    uint2 stack[TRAVERSAL_STACK];
+    bool active = false, exhausted = false;
+    uint32_t item = 0;
+    for (;;) {
+        const uint32_t act = __ballot_sync(0xFFFFFFFFu, active);
+        if (!exhausted && __popc(act) < REFILL_THRESHOLD) {
+            const uint32_t need = ~act;
+            const uint32_t leader = __ffs(need) - 1u;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(work, (uint32_t)__popc(need));
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (!active) {
+                const uint32_t i = base + __popc(need & lt_mask);
+                if (i < n) {
+                    float3 o, d;
+                    float t0, t1;
+                    load(i, o, d, t0, t1);
+                    T.init(S, o, d, t0, t1);
+                    item = i;
+                    active = true;
+                }
+            }
+            if (base + (uint32_t)__popc(need) >= n) exhausted = true;
+        }
+        if (!__any_sync(0xFFFFFFFFu, active)) break;
+        if (active && !T.step(S, tl, in, stack, err)) {
+            store(item, T.res);
+            active = false;
+        }
+    }
+}
+
 template <bool ANY, bool ALPHA>
 LAM_DEV TraceResult trace_ray(const DevScene& S, const uint4* __restrict__ tlas_nodes,
                               const DevInstance* __restrict__ insts, float3 wo, float3 wd, float tmin, float tmax,

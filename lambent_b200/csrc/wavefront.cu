@@ -313,19 +313,18 @@ __global__ void __launch_bounds__(WAVE_BLOCK) extend_kernel(Args A) {
         atomicAdd(A.segments + 1, (unsigned long long)n);  // since the pipeline's buffers were created
     }
     uint32_t err = 0u;
-    for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(A.work, 32u);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= n) break;
-        const uint32_t i = base + lane;
-        if (i >= n) continue;
-        const uint32_t path = A.q_in[i];
-        const float4 o4 = A.ray_o[path], d4 = A.ray_d[path];
-        TraceResult tr = trace_ray<false, ALPHA>(A.S, tl, in, make_float3(o4.x, o4.y, o4.z), make_float3(d4.x, d4.y, d4.z),
-                                                 A.tmin, A.tmax, err);
-        A.hit[path] = make_uint2(tr.tri, tr.inst);
-    }
+    (void)lane;
+    trace_persistent<false, ALPHA>(
+        A.S, tl, in, n, A.work, err,
+        [&](uint32_t i, float3& o, float3& d, float& t0, float& t1) {
+            const uint32_t path = A.q_in[i];
+            const float4 o4 = A.ray_o[path], d4 = A.ray_d[path];
+            o = make_float3(o4.x, o4.y, o4.z);
+            d = make_float3(d4.x, d4.y, d4.z);
+            t0 = A.tmin;
+            t1 = A.tmax;
+        },
+        [&](uint32_t i, const TraceResult& tr) { A.hit[A.q_in[i]] = make_uint2(tr.tri, tr.inst); });
     if (err) atomicOr(A.err, err);
 }
 

@@ -209,22 +209,30 @@ def random_rotation(rng):
                      [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
 
 
+def _interp_matrix(size, g):
+    """(size, g + 1) smoothstep-bilinear weights of lattice points for each pixel row."""
+    coords = np.arange(size, dtype=np.float64) * (g / size)
+    i0 = np.floor(coords).astype(np.int64)
+    fr = coords - i0
+    fr = fr * fr * (3 - 2 * fr)
+    m = np.zeros((size, g + 1), np.float32)
+    m[np.arange(size), i0] = 1 - fr
+    m[np.arange(size), i0 + 1] += fr
+    return m
+
+
 def value_noise(rng, size, octaves=4, base=8, channels=4):
-    out = np.zeros((size, size, channels), np.float32)
+    """Fractal value noise in [0, 1): per octave, a random lattice interpolated as Wy @ L @ Wx^T."""
+    out = np.zeros((channels, size, size), np.float32)
     amp, total = 1.0, 0.0
     for o in range(octaves):
         g = base << o
-        lat = rng.random((g + 1, g + 1, channels)).astype(np.float32)
-        coords = np.arange(size, dtype=np.float32) * (g / size)
-        i0 = np.floor(coords).astype(np.int64)
-        fr = (coords - i0)[:, None]
-        fr = fr * fr * (3 - 2 * fr)
-        rows = lat[i0] * (1 - fr[:, :, None]) + lat[i0 + 1] * fr[:, :, None]          # (size, g+1, C)
-        img = rows[:, i0] * (1 - fr[None, :, :]) + rows[:, i0 + 1] * fr[None, :, :]   # (size, size, C)
-        out += amp * img
+        lat = rng.random((channels, g + 1, g + 1)).astype(np.float32)
+        w = _interp_matrix(size, g)
+        out += amp * np.matmul(np.matmul(w, lat), w.T)
         total += amp
         amp *= 0.5
-    return out / total
+    return np.ascontiguousarray((out / total).transpose(1, 2, 0))
 
 
 def icosphere_field(width=1920, height=1080, instances=64, subdiv=5, tex_size=1024, tex_layers=16, seed=2024):

@@ -65,8 +65,13 @@ def test_reservoirs_and_info_match_oracle(cuda):
     np.testing.assert_allclose(gi, o["buffers"]["info"], atol=1e-5)
     gr = read_buffer(g["buffers"], lb.DataBuffers.RESERVOIRS, np.float32, (P, 16))
     orr = o["buffers"]["reservoirs"]
-    same = np.all(np.isclose(gr, orr, rtol=1e-3, atol=1e-4), axis=1)
-    assert same.mean() > 0.95
+    # words 3, 7, 11, 14 are packed integers (octahedral normals, type, confidence|valid)
+    fcols = [0, 1, 2, 4, 5, 6, 8, 9, 10, 12, 13, 15]
+    icols = [3, 7, 11, 14]
+    gi_, oi_ = gr.view(np.uint32)[:, icols].astype(np.int64), orr.view(np.uint32)[:, icols].astype(np.int64)
+    same_f = np.all(np.isclose(gr[:, fcols], orr[:, fcols], rtol=1e-3, atol=1e-4), axis=1)
+    same_i = np.all(np.abs(gi_ - oi_) <= 1, axis=1) | np.all(gi_ == oi_, axis=1)
+    assert (same_f & same_i).mean() > 0.95, ((same_f & same_i).mean(), same_f.mean(), same_i.mean())
 
 
 def test_statistical_agreement_independent_seeds(cuda):
