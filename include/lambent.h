@@ -380,6 +380,7 @@ int lam_scene_destroy(lam_scene* scene);
 int lam_trace_rays(const lam_scene* scene, const lam_ray* rays, uint32_t n, uint32_t mode,
                    lam_hit* hits, void* stream);
 
+
 /* ---------------------------------------------------------------- DataBuffers */
 /* DataBuffers::new, src/data_buffer/mod.rs:150-252 */
 int lam_data_buffers_new(uint32_t width, uint32_t height, uint32_t world_space_buffer_size,

@@ -83,14 +83,14 @@ LAM_DEV float2 hit_uv(const lam_material& m, float bu, float bv) {
     return make_float2(fmaf(t1.x, bz, fmaf(t2.x, bu, t3.x * bv)), fmaf(t1.y, bz, fmaf(t2.y, bu, t3.y * bv)));
 }
 
-LAM_DEV bool alpha_accept(const DevScene& S, uint32_t inst, uint32_t prim, float bu, float bv) {
+LAM_DEV bool alpha_accept(const DevScene& S, uint32_t inst, uint32_t prim, float bu, float bv, bool transparent_passes) {
     if (S.material_count == 0u) return true;
     lam_material m = load_material(S, inst, prim);
     float2 uv = hit_uv(m, bu, bv);
     uint32_t idx_d = m.tex_idx_diffuse_emission & 0xFFFFu;
     uint32_t ty = m.tex_idx_attributes_ty >> 16;
     float4 px = tex_sample(S, S.diffuse_first, S.diffuse_count, idx_d, uv.x, uv.y);
-    return !near_zero(px.w) || ty == TY_TRANSPARENT;
+    return !near_zero(px.w) || (transparent_passes && ty == TY_TRANSPARENT);
 }
 
 }  // namespace lam

@@ -400,3 +400,4 @@ extern "C" int lam_trace_rays(const lam_scene* s, const lam_ray* rays, uint32_t 
     if (err_flags & ERR_STACK_OVERFLOW) return set_error(LAM_ERR_STACK_OVERFLOW, "traversal stack overflow");
     return LAM_OK;
 }
+

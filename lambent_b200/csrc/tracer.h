@@ -63,4 +63,7 @@ struct lam_pipeline {
 
 namespace lam {
 int set_intersection_handler(lam_tracer* t, const char* src);
+// Debug views (FrontFace / Reflectance / Tangent), debug.cu.
+int render_debug(lam_pipeline* pl, const lam_scene* s, const lam_camera* cam, const lam_frame_targets* tg,
+                 cudaStream_t st);
 }

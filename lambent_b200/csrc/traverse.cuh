@@ -34,7 +34,13 @@ LAM_DEV float sel3(int k, float x, float y, float z) { return k == 0 ? x : (k ==
 
 LAM_DEV float safe_rcp(float x) {
     float y = fabsf(x) < 1e-30f ? copysignf(1e-30f, x) : x;
+#ifdef LAM_FAST_RCP
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(y));
+    return r;
+#else
     return __frcp_rn(y);
+#endif
 }
 
 LAM_DEV void setup_ray(TravRay& r, float3 o, float3 d) {
@@ -156,9 +162,19 @@ LAM_DEV float qbyte(uint32_t w, uint32_t k) {
 
 // Intersects the 8 children of one node.  Outputs the node group (child_base, internal hits in
 // bits 24..31 in octant order | imask) and the leaf group (leaf_base, item hits in bits 0..23).
+template <bool GLOBAL>
+LAM_DEV uint4 load_node_word(const uint4* p) {
+#ifdef LAM_NC_NODES
+    if (GLOBAL) return __ldg(p);
+#endif
+    return *p;
+}
+
+template <bool GLOBAL = false>
 LAM_DEV void intersect_node(const uint4* __restrict__ np, const TravRay& r, float tmin, float tmax, uint2& ng,
                             uint2& tg) {
-    const uint4 n0 = np[0], n1 = np[1], n2 = np[2], n3 = np[3], n4 = np[4];
+    const uint4 n0 = load_node_word<GLOBAL>(np), n1 = load_node_word<GLOBAL>(np + 1), n2 = load_node_word<GLOBAL>(np + 2),
+                n3 = load_node_word<GLOBAL>(np + 3), n4 = load_node_word<GLOBAL>(np + 4);
     const float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
     const uint32_t imask = n0.w >> 24;
     const float sx = __uint_as_float((n0.w & 0xFFu) << 23);
@@ -207,7 +223,7 @@ struct TraceResult {
 
 // Alpha-test callback for non-opaque geometry: candidate accepted unless the diffuse texel's
 // alpha is near zero, transparent materials always accepted (general.wesl:1059-1067).
-LAM_DEV bool alpha_accept(const DevScene& S, uint32_t inst, uint32_t prim, float bu, float bv);
+LAM_DEV bool alpha_accept(const DevScene& S, uint32_t inst, uint32_t prim, float bu, float bv, bool transparent_passes);
 
 // Resumable traversal: init() then step() until it returns false.  One step intersects one node
 // and tests the leaf items it exposes, so a warp can refill lanes whose rays have finished
@@ -221,6 +237,7 @@ struct Traverser {
     int sp, blas_base;
     uint32_t cur_inst, cur_flags;
     TraceResult res;
+    bool transparent_passes = true;  // transparent materials pass the alpha test (path shaders)
 
     LAM_DEV void init(const DevScene& S, float3 o, float3 d, float t0, float t1) {
         wo = o;
@@ -256,13 +273,22 @@ struct Traverser {
             const uint32_t slot = k ^ R.oct;
             const uint32_t child = ng.x + __popc(ng.y & ((1u << slot) - 1u) & 0xFFu);
             if (ng.y > 0x00FFFFFFu) push(stack, ng, err);
-            const uint4* nodes = blas_base < 0 ? tlas_nodes : S.blas_nodes;
-            intersect_node(nodes + 5u * child, R, tmin, best_t, ng, tg);
+            if (blas_base < 0) intersect_node<false>(tlas_nodes + 5u * child, R, tmin, best_t, ng, tg);
+            else intersect_node<true>(S.blas_nodes + 5u * child, R, tmin, best_t, ng, tg);
         } else {
             tg = ng;
             ng = make_uint2(0u, 0u);
         }
         while (tg.y != 0u) {
+#ifdef LAM_POSTPONE
+            // Postpone only while this lane still has node work: the postponed group comes back
+            // once the node work is exhausted, and is then always processed (no livelock).
+            if (blas_base >= 0 && ng.y > 0x00FFFFFFu && __popc(__activemask()) < LAM_POSTPONE) {
+                push(stack, tg, err);
+                tg.y = 0u;
+                break;
+            }
+#endif
             const uint32_t k = __ffs(tg.y) - 1u;
             tg.y &= tg.y - 1u;
             const uint32_t item = tg.x + k;
@@ -299,7 +325,7 @@ struct Traverser {
                 float rt, ru, rv;
                 bool fr;
                 wbw_f64(R.o, R.d, a, b, c, &rt, &ru, &rv, &fr);
-                if (!alpha_accept(S, cur_inst, prim, ru, rv)) continue;
+                if (!alpha_accept(S, cur_inst, prim, ru, rv, transparent_passes)) continue;
             }
             best_t = t;
             res.tri = item;
@@ -327,7 +353,7 @@ struct Traverser {
 
 // Lanes below this many active rays trigger a refill of the idle lanes from the work queue.
 #ifndef LAM_REFILL_THRESHOLD
-#define LAM_REFILL_THRESHOLD 20
+#define LAM_REFILL_THRESHOLD 24
 #endif
 constexpr int REFILL_THRESHOLD = LAM_REFILL_THRESHOLD;
 
@@ -371,109 +397,6 @@ LAM_DEV void trace_persistent(const DevScene& S, const uint4* __restrict__ tl, c
     }
 }
 
-template <bool ANY, bool ALPHA>
-LAM_DEV TraceResult trace_ray(const DevScene& S, const uint4* __restrict__ tlas_nodes,
-                              const DevInstance* __restrict__ insts, float3 wo, float3 wd, float tmin, float tmax,
-                              uint32_t& err) {
-    TraceResult res;
-    res.tri = NO_HIT;
-    res.inst = NO_HIT;
-    res.prim = NO_HIT;
-    res.t = tmax;
-    if (S.tlas_node_count == 0u) return res;
-    float best_t = tmax;
-    TravRay R;
-    setup_ray(R, wo, wd);
-    uint2 stack[TRAVERSAL_STACK];
-    int sp = 0;
-    int blas_base = -1;
-    uint32_t cur_inst = 0u, cur_flags = 0u;
-    const uint4* __restrict__ nodes = tlas_nodes;
-    uint2 ng = make_uint2(0u, (1u << (24u + R.oct)) | 1u);
-    uint2 tg = make_uint2(0u, 0u);
-    for (;;) {
-        if (ng.y > 0x00FFFFFFu) {
-            const uint32_t k = __ffs(ng.y >> 24) - 1u;
-            ng.y &= ~(1u << (24u + k));
-            const uint32_t slot = k ^ R.oct;
-            const uint32_t child = ng.x + __popc(ng.y & ((1u << slot) - 1u) & 0xFFu);
-            if (ng.y > 0x00FFFFFFu) {
-                if (sp < TRAVERSAL_STACK) stack[sp++] = ng;
-                else err |= ERR_STACK_OVERFLOW;
-            }
-            intersect_node(nodes + 5u * child, R, tmin, best_t, ng, tg);
-        } else {
-            tg = ng;
-            ng = make_uint2(0u, 0u);
-        }
-        while (tg.y != 0u) {
-            const uint32_t k = __ffs(tg.y) - 1u;
-            tg.y &= tg.y - 1u;
-            const uint32_t item = tg.x + k;
-            if (blas_base < 0) {
-                const uint32_t id = __ldg(S.tlas_items + item);
-                const DevInstance& I = insts[id];
-                const uint32_t flags = I.flags;
-                const uint32_t root = I.blas_root;
-                if (!(flags & INST_VISIBLE) || root == NO_HIT) continue;
-                if (tg.y != 0u) {
-                    if (sp < TRAVERSAL_STACK) stack[sp++] = tg;
-                    else err |= ERR_STACK_OVERFLOW;
-                }
-                if (ng.y > 0x00FFFFFFu) {
-                    if (sp < TRAVERSAL_STACK) stack[sp++] = ng;
-                    else err |= ERR_STACK_OVERFLOW;
-                }
-                blas_base = sp;
-                cur_inst = id;
-                cur_flags = flags;
-                nodes = S.blas_nodes;
-                float m[12];
-#pragma unroll
-                for (int q = 0; q < 12; ++q) m[q] = I.inv[q];
-                float3 oo, od;
-                object_ray(m, wo, wd, &oo, &od);
-                setup_ray(R, oo, od);
-                ng = make_uint2(root, (1u << (24u + R.oct)) | 1u);
-                tg = make_uint2(0u, 0u);
-                break;
-            }
-            const float4* tp = S.tris + 3u * item;
-            const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-            float t;
-            if (!wbw_f32(R, a, b, c, best_t, &t)) continue;
-            const uint32_t prim = __float_as_uint(a.w);
-            bool better = t > tmin && (t < best_t || (t == best_t && res.tri != NO_HIT &&
-                                                      (cur_inst < res.inst || (cur_inst == res.inst && prim < res.prim))));
-            if (!better) continue;
-            if (ALPHA && !(cur_flags & INST_OPAQUE)) {
-                float rt, ru, rv;
-                bool fr;
-                wbw_f64(R.o, R.d, a, b, c, &rt, &ru, &rv, &fr);
-                if (!alpha_accept(S, cur_inst, prim, ru, rv)) continue;
-            }
-            best_t = t;
-            res.tri = item;
-            res.inst = cur_inst;
-            res.prim = prim;
-            if (ANY) {
-                res.t = best_t;
-                return res;
-            }
-        }
-        if (ng.y <= 0x00FFFFFFu && tg.y == 0u) {
-            if (blas_base >= 0 && sp == blas_base) {
-                blas_base = -1;
-                nodes = tlas_nodes;
-                setup_ray(R, wo, wd);
-            }
-            if (sp == 0) break;
-            ng = stack[--sp];
-        }
-    }
-    res.t = best_t;
-    return res;
-}
 
 constexpr int TRACE_BLOCK = 128;
 constexpr uint32_t SMEM_TLAS_NODES = 64;   // TLAS staged in shared memory when it fits

@@ -885,7 +885,8 @@ extern "C" int lam_tracer_create_pipeline(const lam_tracer* t, const lam_pipelin
     if (o->restir_temporal > LAM_RESTIR_PER_PIXEL) return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown ReSTIR mode");
     if (o->guide_mode > LAM_GUIDE_LEARNED) return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown guide mode");
     if (o->guide_mode == LAM_GUIDE_LEARNED) return set_error(LAM_ERR_UNSUPPORTED, "learned guiding is not available in this pipeline");
-    if (t->quality > LAM_QUALITY_HIGH) return set_error(LAM_ERR_UNSUPPORTED, "debug shaders are rendered with lam_render_debug");
+    if (t->quality > LAM_QUALITY_HIGH && (t->quality < LAM_DEBUG_FRONT_FACE || t->quality > LAM_DEBUG_TANGENT))
+        return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown shader");
     lam_pipeline* p = new lam_pipeline();
     p->quality = t->quality;
     p->opts = *o;
@@ -981,6 +982,7 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
     if (s->instance_count > pl->layout.blas_count || s->diffuse_count > pl->layout.diffuse_count ||
         s->emission_count > pl->layout.emission_count || s->attribute_count > pl->layout.attribute_count)
         return set_error(LAM_ERR_LAYOUT_MISMATCH, "scene bindings exceed the pipeline layout counts");
+    if (pl->quality >= LAM_DEBUG_FRONT_FACE) return render_debug(pl, s, cam, tg, (cudaStream_t)stream);
     const bool guide = pl->opts.guide_mode == LAM_GUIDE_MARKOV;
     const uint32_t restir = pl->opts.restir_temporal;
     const bool full = guide || restir != LAM_RESTIR_DISABLED;

@@ -948,8 +948,45 @@ struct PT {
 
 }  // namespace
 
+// Debug views, src/debug/{front_face,reflectance,tangent}.wesl: one primary ray per pixel.  The
+// candidate test of these shaders keeps only triangles whose diffuse alpha is not near zero
+// (no exception for transparent materials); the oracle's scene marks every BLAS opaque or not,
+// and debug renders of non-opaque geometry use the same alpha rule as the path shaders here.
+static int render_debug(const Scene& sc, const RenderParams& p, RenderCounters* counters) {
+    PT pt(sc, p);
+    for (uint32_t y = 0; y < p.height; ++y) {
+        for (uint32_t x = 0; x < p.width; ++x) {
+            Ray r = pt.create_ray(x, y);
+            Hit h = sc.trace(r.origin, r.direction, p.tmin, p.tmax, false);
+            vec3 c(0.0f);
+            if (p.quality == LAM_DEBUG_TANGENT) {
+                vec3 dir = h.hit ? normalize(h.ov0 - h.ov1) : vec3(0.0f);
+                c = (correct_tangent(dir) + vec3(1.0f)) / 2.0f;
+            } else if (h.hit && p.quality == LAM_DEBUG_FRONT_FACE) {
+                float g = 1.0f / (h.t + 1.0f);
+                c = h.front ? vec3(0.0f, g, 0.0f) : vec3(g, 0.0f, 0.0f);
+            } else if (h.hit) {
+                // reflectance.wesl:88 reads material_idx[geometry_index], i.e. instance 0's table
+                const lam_material& m = pt.material_of(0, h.prim);
+                vec2 ior = unpack2x16float(m.refractive_index);
+                c = vec3(ior.x / 5.0f, ior.y / 5.0f, 0.0f);
+            }
+            uint64_t idx = (uint64_t)x + (uint64_t)y * p.width;
+            if (p.out_color) PT::st4(p.out_color, idx, c);
+            if (p.out_normal) PT::st4(p.out_normal, idx, vec3(0.0f));
+            if (p.out_albedo) PT::st4(p.out_albedo, idx, vec3(0.0f));
+        }
+    }
+    if (counters) {
+        counters->segments = (uint64_t)p.width * p.height;
+        counters->samples = counters->segments;
+    }
+    return LAM_OK;
+}
+
 int render(const Scene& scene, const RenderParams& p, RenderCounters* counters) {
     if (p.width == 0 || p.height == 0 || p.samples == 0) return LAM_ERR_INVALID_ARGUMENT;
+    if (p.quality >= LAM_DEBUG_FRONT_FACE) return render_debug(scene, p, counters);
     uint32_t y0 = p.crop_w ? p.crop_y0 : 0u;
     uint32_t y1 = p.crop_w ? std::min(p.height, p.crop_y0 + p.crop_h) : p.height;
     uint32_t x0 = p.crop_w ? (p.crop_x0 / SUBGROUP) * SUBGROUP : 0u;

@@ -111,3 +111,13 @@ def test_depth_and_layout_errors(cuda):
     with pytest.raises(lb.LambentError) as e:
         pipe.render(lb.GpuScene(s), lb.DataBuffers(16, 16, 16, 7), s.camera, lb.targets_from(col))
     assert e.value.code == _abi.ERR_LAYOUT_MISMATCH
+
+
+@pytest.mark.parametrize("mode", [_abi.DEBUG_FRONT_FACE, _abi.DEBUG_REFLECTANCE, _abi.DEBUG_TANGENT])
+def test_debug_views_match_oracle(cuda, mode):
+    """The reference's debugging shaders (src/debug/*.wesl) as kernels over the same traversal."""
+    s = scenes.unit_cube_scene(64, 64)
+    g = gpu_render(s, 1, quality=mode, restir=_abi.RESTIR_DISABLED)
+    o = O.OracleScene(s).render(s.camera, 64, 64, samples=1, quality=mode, restir=_abi.RESTIR_DISABLED)
+    np.testing.assert_allclose(g["color"], o["color"], rtol=1e-5, atol=1e-6)
+    assert (g["normal"][..., :3] == 0).all()
