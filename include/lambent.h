@@ -380,6 +380,18 @@ int lam_scene_destroy(lam_scene* scene);
 int lam_trace_rays(const lam_scene* scene, const lam_ray* rays, uint32_t n, uint32_t mode,
                    lam_hit* hits, void* stream);
 
+/* Allocation-free form of lam_trace_rays; it has no counterpart in the reference.  For callers
+ * that cannot allocate device memory while they run (a render loop inside a fixed frame budget,
+ * where cudaMalloc/cudaFree can synchronise the device, or a host that reserves all of its GPU
+ * memory up front): the query's scratch (a work counter and error flags) lives in a 256-byte
+ * static device array that every GPU loading this library keeps until the process exits.
+ * n must not exceed LAM_TRACE_STATIC_MAX_RAYS (larger n: LAM_ERR_INVALID_ARGUMENT).  All calls
+ * share that array: calls that overlap on the GPU race and must be serialised.  The first call on
+ * a device looks up the array's device address; make it before any stream capture.  The current
+ * device must be the scene's.  Results are identical to lam_trace_rays. */
+#define LAM_TRACE_STATIC_MAX_RAYS 0x7FFFFFFFu
+int lam_trace_rays_static(const lam_scene* scene, const lam_ray* rays, uint32_t n, uint32_t mode,
+                          lam_hit* hits, void* stream);
 
 /* ---------------------------------------------------------------- DataBuffers */
 /* DataBuffers::new, src/data_buffer/mod.rs:150-252 */

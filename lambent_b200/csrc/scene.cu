@@ -401,3 +401,87 @@ extern "C" int lam_trace_rays(const lam_scene* s, const lam_ray* rays, uint32_t 
     return LAM_OK;
 }
 
+// ---------------------------------------------------------------- allocation-free ray query
+//
+// lam_trace_rays_static: the same closest-hit / any-hit query as lam_trace_rays for callers that
+// must not allocate device memory while they run (for example a render loop inside a fixed frame
+// budget, where cudaMalloc / cudaFree can synchronise the device and stall the frame, or a host
+// that reserves all of its GPU memory up front and forbids allocations afterwards).  Its only
+// scratch - the work counter that hands rays to warps and the error flags - lives in the
+// file-scope array below, which every GPU that loads this library holds until the process exits.
+//
+// Limits and sharing:
+//   * n <= LAM_TRACE_STATIC_MAX_RAYS (2^31 - 1): the 32-bit work counter may overshoot n by one
+//     claim per warp of the grid and must not wrap;
+//   * every call uses the same array: calls that overlap on the GPU (different streams, or
+//     several host threads) race on the counter and give wrong results; serialise them;
+//   * the array keeps the last call's contents; each call clears the two words it uses first;
+//   * the first call on a device resolves the array's device address with cudaGetSymbolAddress
+//     (once per device); make that first call before any stream capture.
+namespace lam {
+
+constexpr uint32_t STATIC_TRACE_WORDS = 64;  // 256 bytes; words 0 (work counter) and 1 (error flags) used
+static __device__ __align__(256) uint32_t g_static_trace_scratch[STATIC_TRACE_WORDS];
+
+constexpr int STATIC_TRACE_MAX_DEVICES = 64;
+static std::atomic<uint32_t*> g_static_trace_ptr[STATIC_TRACE_MAX_DEVICES];
+
+// Device address of g_static_trace_scratch on `device` (the current device); resolved once.
+static int static_trace_scratch(int device, uint32_t** out) {
+    if (device < 0 || device >= STATIC_TRACE_MAX_DEVICES)
+        return set_error(LAM_ERR_UNSUPPORTED, "lam_trace_rays_static: device index beyond 63");
+    uint32_t* p = g_static_trace_ptr[device].load(std::memory_order_acquire);
+    if (!p) {
+        void* addr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&addr, g_static_trace_scratch);
+        if (e != cudaSuccess) return cuda_error(e, "lam_trace_rays_static: cudaGetSymbolAddress");
+        p = static_cast<uint32_t*>(addr);
+        g_static_trace_ptr[device].store(p, std::memory_order_release);
+    }
+    *out = p;
+    return LAM_OK;
+}
+
+}  // namespace lam
+
+extern "C" int lam_trace_rays_static(const lam_scene* s, const lam_ray* rays, uint32_t n, uint32_t mode,
+                                     lam_hit* hits, void* stream) {
+    if (!s || (n && (!rays || !hits))) return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_trace_rays_static: null argument");
+    if (mode != LAM_TRACE_CLOSEST && mode != LAM_TRACE_ANY)
+        return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_trace_rays_static: unknown mode");
+    if (n > LAM_TRACE_STATIC_MAX_RAYS)
+        return set_error(LAM_ERR_INVALID_ARGUMENT,
+                         "lam_trace_rays_static: n exceeds LAM_TRACE_STATIC_MAX_RAYS (2^31 - 1 rays per call)");
+    if (n == 0) return LAM_OK;
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return cuda_error(e, "lam_trace_rays_static: cudaGetDevice");
+    if (device != s->device)
+        return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_trace_rays_static: the current device is not the scene's");
+    uint32_t* scratch = nullptr;
+    int rc = static_trace_scratch(device, &scratch);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    e = cudaMemsetAsync(scratch, 0, 2 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return cuda_error(e, "lam_trace_rays_static: clearing the scratch words");
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    dim3 grid(sms * 8), block(TRACE_BLOCK);
+    const bool alpha = !s->dev.all_opaque;
+    if (mode == LAM_TRACE_ANY) {
+        if (alpha) trace_rays_kernel<true, true><<<grid, block, 0, st>>>(s->dev, rays, n, hits, scratch, scratch + 1);
+        else trace_rays_kernel<true, false><<<grid, block, 0, st>>>(s->dev, rays, n, hits, scratch, scratch + 1);
+    } else {
+        if (alpha) trace_rays_kernel<false, true><<<grid, block, 0, st>>>(s->dev, rays, n, hits, scratch, scratch + 1);
+        else trace_rays_kernel<false, false><<<grid, block, 0, st>>>(s->dev, rays, n, hits, scratch, scratch + 1);
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_error(e, "lam_trace_rays_static: launch");
+    uint32_t err_flags = 0;
+    e = cudaMemcpyAsync(&err_flags, scratch + 1, sizeof(err_flags), cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_error(e, "lam_trace_rays_static: reading the error flags");
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_error(e, "lam_trace_rays_static");
+    if (err_flags & ERR_STACK_OVERFLOW) return set_error(LAM_ERR_STACK_OVERFLOW, "traversal stack overflow");
+    return LAM_OK;
+}
