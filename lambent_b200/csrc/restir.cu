@@ -167,7 +167,6 @@ __global__ void eof_world_kernel(uint32_t* world, uint64_t n) {
     e[W_TIMEOUT] = e[W_TIMEOUT] - 1u;
 }
 
-constexpr int MAX_AVERAGE_FRAMES = 1024;
 struct FramePtrs {
     const float4* f[64];
 };

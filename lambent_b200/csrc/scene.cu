@@ -182,18 +182,24 @@ extern "C" int lam_scene_create(const lam_scene_desc* d, void* stream, lam_scene
         bool opaque = (d->blas[id.blas].flags & LAM_GEOMETRY_OPAQUE) != 0u;
         all_opaque = all_opaque && opaque;
         I.flags = (opaque ? INST_OPAQUE : 0u) | ((id.mask & 0xFFu) ? INST_VISIBLE : 0u);
-        // world box of the transformed BLAS bounds, rounded outward with a relative pad
+        // exact world box of the instance's transformed vertices (FP64), padded outward; a box of the
+        // rotated object-space bounds would be up to 3^1.5 times larger and admit many rays that
+        // cannot hit the instance
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-        const Bvh8& bv = bvh[id.blas];
-        for (int c = 0; c < 8; ++c) {
-            double p[3] = {(c & 1) ? bv.hi[0] : bv.lo[0], (c & 2) ? bv.hi[1] : bv.lo[1], (c & 4) ? bv.hi[2] : bv.lo[2]};
+        const lam_blas_desc& bd = d->blas[id.blas];
+        const uint32_t nidx = tri_count[id.blas] * 3u;
+        for (uint32_t k = 0; k < nidx; ++k) {
+            const uint32_t vi = bd.indices ? bd.indices[k] : k;
+            const float* pv = bd.vertices + (size_t)vi * bd.vertex_stride;
             for (int r = 0; r < 3; ++r) {
                 const float* q = id.transform + 4 * r;
-                double w = (double)q[0] * p[0] + (double)q[1] * p[1] + (double)q[2] * p[2] + (double)q[3];
+                double w = (double)q[0] * pv[0] + (double)q[1] * pv[1] + (double)q[2] * pv[2] + (double)q[3];
                 lo[r] = std::min(lo[r], w);
                 hi[r] = std::max(hi[r], w);
             }
         }
+        if (nidx == 0)
+            for (int r = 0; r < 3; ++r) lo[r] = hi[r] = (double)id.transform[4 * r + 3];
         double mag = 0.0;
         for (int k = 0; k < 3; ++k) mag = std::max({mag, std::fabs(lo[k]), std::fabs(hi[k]), hi[k] - lo[k]});
         double pad = mag * 1e-5 + 1e-30;

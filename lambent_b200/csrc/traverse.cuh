@@ -34,13 +34,11 @@ LAM_DEV float sel3(int k, float x, float y, float z) { return k == 0 ? x : (k ==
 
 LAM_DEV float safe_rcp(float x) {
     float y = fabsf(x) < 1e-30f ? copysignf(1e-30f, x) : x;
-#ifdef LAM_FAST_RCP
+    // approximate reciprocal (<= 1 ulp): the slab distances only need to be conservative, which the
+    // 2^-20 far-distance margin and the one-step box padding guarantee
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(y));
     return r;
-#else
-    return __frcp_rn(y);
-#endif
 }
 
 LAM_DEV void setup_ray(TravRay& r, float3 o, float3 d) {
@@ -164,9 +162,6 @@ LAM_DEV float qbyte(uint32_t w, uint32_t k) {
 // bits 24..31 in octant order | imask) and the leaf group (leaf_base, item hits in bits 0..23).
 template <bool GLOBAL>
 LAM_DEV uint4 load_node_word(const uint4* p) {
-#ifdef LAM_NC_NODES
-    if (GLOBAL) return __ldg(p);
-#endif
     return *p;
 }
 
@@ -280,15 +275,6 @@ struct Traverser {
             ng = make_uint2(0u, 0u);
         }
         while (tg.y != 0u) {
-#ifdef LAM_POSTPONE
-            // Postpone only while this lane still has node work: the postponed group comes back
-            // once the node work is exhausted, and is then always processed (no livelock).
-            if (blas_base >= 0 && ng.y > 0x00FFFFFFu && __popc(__activemask()) < LAM_POSTPONE) {
-                push(stack, tg, err);
-                tg.y = 0u;
-                break;
-            }
-#endif
             const uint32_t k = __ffs(tg.y) - 1u;
             tg.y &= tg.y - 1u;
             const uint32_t item = tg.x + k;
