@@ -60,8 +60,8 @@ enum { LAM_RESTIR_DISABLED = 0, LAM_RESTIR_PER_SAMPLE = 1, LAM_RESTIR_PER_PIXEL 
  * LAM_GUIDE_NONE    - BSDF (cosine) sampling only: the branch the reference takes when no
  *                     Markov chain is valid (src/path_tracing/general.wesl:812-815).
  * LAM_GUIDE_MARKOV  - the reference's vMF Markov-chain mixture (general.wesl:764-866).
- * LAM_GUIDE_LEARNED - Markov/BSDF sampler combined with the learned lobe mixture by
- *                     one-sample MIS (no counterpart in the reference). */
+ * LAM_GUIDE_LEARNED - cosine BSDF sampler combined with the learned lobe mixture by
+ *                     one-sample MIS (no counterpart in the reference; see lam_guide). */
 enum { LAM_GUIDE_NONE = 0, LAM_GUIDE_MARKOV = 1, LAM_GUIDE_LEARNED = 2 };
 
 /* BufferType bitflags, src/data_buffer/mod.rs:18-27 */
@@ -263,11 +263,12 @@ typedef struct lam_render_stats {
 typedef struct lam_stage_times {
     double generate_ms;
     double extend_ms;
-    double shade_ms;
+    double shade_ms;           /* shade + learned-guide sampling */
     double accumulate_ms;      /* accumulate + chain shuffle */
     uint64_t extend_launches;
     uint64_t shade_launches;
     uint64_t ray_segments;     /* segments traced by the timed renders */
+    double train_ms;           /* learned-guide training steps */
 } lam_stage_times;
 
 /* Opaque handles */
@@ -428,6 +429,71 @@ int lam_temporal_resampling(lam_data_buffers* buffers, uint32_t width, uint32_t 
 int lam_spatial_resampling(lam_data_buffers* buffers, const lam_frame_targets* targets,
                            uint32_t is_samples, uint32_t is_space, uint32_t seed_offset,
                            void* stream);
+
+/* ---------------------------------------------------------------- learned path guiding
+ * No counterpart in the reference (its guiding is the Markov-chain cache, general.wesl:764-866).
+ * A 4-layer MLP (64 wide, BF16 weights, FP32 accumulation on the tensor cores) maps a diffuse
+ * vertex (position, normal, outgoing direction) to an 8-lobe vMF mixture over incident directions.
+ * With guide_mode LAM_GUIDE_LEARNED and a guide attached to the pipeline, lam_render samples
+ * that mixture with probability guide_fraction and the cosine BSDF lobe otherwise, and weights
+ * the sample by the mixture pdf (one-sample MIS, balance heuristic): the estimate stays unbiased.
+ * While fewer than train_spp samples per pixel have been rendered with the guide, every render
+ * records its diffuse vertices (and the radiance their paths carried back) and takes
+ * steps_per_wave Adam steps on them after each wave of samples.  Until the first training step
+ * the guided render is the plain one, sample for sample.
+ *
+ * Parameters (lam_guide_get_params / set_params) are 4 x 64 x 64 f32, W[layer][out][in]:
+ * layer input column 63 is the constant 1 (so W[l][o][63] is the bias), hidden unit 63 is that
+ * constant (rows W[0..2][63][*] are unused), and head rows 40..63 are unused.  Head outputs:
+ * 0-7 mixture logits, 8-15 log concentration (clamped to [-3, 6]), 16-23 / 24-31 / 32-39 the
+ * x / y / z components of the (normalised) lobe means. */
+#define LAM_GUIDE_PARAMS 16384u
+#define LAM_GUIDE_OUTPUTS 40u
+typedef struct lam_guide lam_guide;
+typedef struct lam_guide_options {
+    uint32_t train_spp;        /* samples per pixel that train the network (default 32) */
+    uint32_t steps_per_wave;   /* Adam steps after each wave of training samples (default 32) */
+    uint32_t batch;            /* training records per step, a multiple of 128 (default 16384) */
+    uint32_t record_capacity;  /* training records kept per wave (default 2^21) */
+    float learning_rate;       /* Adam step size (default 2e-3) */
+    float guide_fraction;      /* probability of sampling the learned mixture (default 0.5) */
+    uint32_t seed;             /* weight initialisation and minibatch selection */
+} lam_guide_options;
+/* A query: position, shading normal, outgoing direction (toward the previous vertex). */
+typedef struct lam_guide_query {
+    float pos[3], normal[3], wo[3];
+} lam_guide_query;
+/* A training record: a query, the sampled incident direction wi and the weight of -log q(wi):
+ * the luminance of (BSDF * cos * incident radiance / pdf) the path carried back. */
+typedef struct lam_guide_record {
+    float pos[3], normal[3], wo[3], wi[3];
+    float weight;
+} lam_guide_record;
+
+int lam_guide_options_default(lam_guide_options* out);
+int lam_guide_create(const lam_guide_options* options, lam_guide** out);
+int lam_guide_destroy(lam_guide* guide);
+/* Host copies of the f32 master parameters.  set_params also resets the Adam state and the
+ * count of trained samples. */
+int lam_guide_get_params(const lam_guide* guide, float* params);
+int lam_guide_set_params(lam_guide* guide, const float* params);
+/* Raw head outputs (n x 40 f32, device) for n device queries; box = scene bounds lo xyz, hi xyz
+ * (lam_scene_bounds) used to normalise positions. */
+int lam_guide_eval(const lam_guide* guide, const lam_guide_query* queries, uint32_t n, const float box[6],
+                   float* outputs, void* stream);
+/* Loss  (1/n) sum -weight log q(wi)  and its gradient with respect to the parameters (f32, device,
+ * LAM_GUIDE_PARAMS entries, zero for unused ones) over n device records. */
+int lam_guide_loss_grad(lam_guide* guide, const lam_guide_record* records, uint32_t n, const float box[6],
+                        float* grad, float* loss, void* stream);
+/* steps Adam steps on minibatches of options.batch records drawn from the n device records. */
+int lam_guide_train(lam_guide* guide, const lam_guide_record* records, uint32_t n, uint32_t steps,
+                    const float box[6], void* stream);
+/* Number of Adam steps taken and samples per pixel trained so far. */
+int lam_guide_progress(const lam_guide* guide, uint64_t* steps, uint32_t* trained_spp);
+/* Attaches the guide used by lam_render when guide_mode is LAM_GUIDE_LEARNED (NULL detaches). */
+int lam_pipeline_set_guide(lam_pipeline* pipeline, lam_guide* guide);
+/* World-space bounds of the scene's geometry: lo xyz, hi xyz. */
+int lam_scene_bounds(const lam_scene* scene, float box[6]);
 
 /* average, examples/cornell_box/src/average_to_buf.wgsl:11-21: out_rgb[3*p+c] = mean over
  * the n rgba32f device images frames[0..n) (host array of device pointers). */

@@ -126,7 +126,16 @@ class RenderStats(C.Structure):
 class StageTimes(C.Structure):
     _fields_ = [("generate_ms", C.c_double), ("extend_ms", C.c_double), ("shade_ms", C.c_double),
                 ("accumulate_ms", C.c_double), ("extend_launches", u64), ("shade_launches", u64),
-                ("ray_segments", u64)]
+                ("ray_segments", u64), ("train_ms", C.c_double)]
+
+
+class GuideOptions(C.Structure):
+    _fields_ = [("train_spp", u32), ("steps_per_wave", u32), ("batch", u32), ("record_capacity", u32),
+                ("learning_rate", C.c_float), ("guide_fraction", C.c_float), ("seed", u32)]
+
+
+GUIDE_PARAMS = 16384
+GUIDE_OUTPUTS = 40
 
 
 class RawTextures(C.Structure):

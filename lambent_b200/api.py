@@ -90,6 +90,17 @@ def lib():
     _sig(L, "lam_temporal_resampling", i, vp, u32, u32, u32, vp)
     _sig(L, "lam_spatial_resampling", i, vp, P(FrameTargets), u32, u32, u32, vp)
     _sig(L, "lam_average_frames", i, P(vp), u32, u32, u32, vp, vp)
+    _sig(L, "lam_guide_options_default", i, P(_abi.GuideOptions))
+    _sig(L, "lam_guide_create", i, P(_abi.GuideOptions), P(vp))
+    _sig(L, "lam_guide_destroy", i, vp)
+    _sig(L, "lam_guide_get_params", i, vp, f32p)
+    _sig(L, "lam_guide_set_params", i, vp, f32p)
+    _sig(L, "lam_guide_eval", i, vp, vp, u32, f32p, vp, vp)
+    _sig(L, "lam_guide_loss_grad", i, vp, vp, u32, f32p, vp, vp, vp)
+    _sig(L, "lam_guide_train", i, vp, vp, u32, u32, f32p, vp)
+    _sig(L, "lam_guide_progress", i, vp, P(C.c_uint64), u32p)
+    _sig(L, "lam_pipeline_set_guide", i, vp, vp)
+    _sig(L, "lam_scene_bounds", i, vp, f32p)
     _LIB = L
     return L
 
@@ -407,6 +418,11 @@ class Pipeline:
     def profile_reset(self):
         check(lib().lam_render_profile_reset(self._h))
 
+    def set_guide(self, guide):
+        """Attaches a learned Guide (used when the options' guide_mode is GuideMode.LEARNED)."""
+        self._guide = guide
+        check(lib().lam_pipeline_set_guide(self._h, guide._h if guide is not None else None))
+
     def __del__(self):
         if getattr(self, "_h", None) and _LIB is not None:
             _LIB.lam_pipeline_destroy(self._h)
@@ -434,6 +450,12 @@ class GpuScene:
         s = SceneStats()
         check(lib().lam_scene_stats_get(self._h, C.byref(s)))
         return s
+
+    def bounds(self):
+        """World-space bounds of the geometry: (lo xyz, hi xyz)."""
+        b = (C.c_float * 6)()
+        check(lib().lam_scene_bounds(self._h, b))
+        return list(b)
 
     def update_materials(self, materials, stream=None):
         arr = (_CMaterial * len(materials))(*materials)
@@ -517,3 +539,65 @@ def average_frames(frames, out_rgb, stream=None):
     h, w = f0.shape[0], f0.shape[1]
     ptrs = (C.c_void_p * len(frames))(*[f.data_ptr() for f in frames])
     check(lib().lam_average_frames(ptrs, len(frames), w, h, C.c_void_p(out_rgb.data_ptr()), _stream_ptr(stream)))
+
+
+# ---------------------------------------------------------------- learned path guiding (no reference counterpart)
+class GuideOptions:
+    """Mirror of lam_guide_options (defaults from lam_guide_options_default)."""
+
+    def __init__(self, **kw):
+        o = _abi.GuideOptions()
+        check(lib().lam_guide_options_default(C.byref(o)))
+        for k, v in kw.items():
+            if not hasattr(o, k):
+                raise AttributeError(k)
+            setattr(o, k, v)
+        self.c = o
+
+
+def _fbox(box):
+    return (C.c_float * 6)(*[float(v) for v in box])
+
+
+class Guide:
+    """The learned guiding network: 4 x 64 x 64 parameters, tcgen05 evaluation and training."""
+
+    def __init__(self, options=None):
+        self.options = options or GuideOptions()
+        h = C.c_void_p()
+        check(lib().lam_guide_create(C.byref(self.options.c), C.byref(h)))
+        self._h = h
+
+    def params(self):
+        out = (C.c_float * _abi.GUIDE_PARAMS)()
+        check(lib().lam_guide_get_params(self._h, out))
+        return list(out)
+
+    def set_params(self, params):
+        arr = (C.c_float * _abi.GUIDE_PARAMS)(*[float(v) for v in params])
+        check(lib().lam_guide_set_params(self._h, arr))
+
+    def eval(self, queries, box, out, stream=None):
+        """queries: CUDA float32 (n, 9) = pos, normal, wo; out: CUDA float32 (n, 40) head outputs."""
+        check(lib().lam_guide_eval(self._h, C.c_void_p(queries.data_ptr()), queries.shape[0], _fbox(box),
+                                   C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
+
+    def loss_grad(self, records, box, grad, loss, stream=None):
+        """records: CUDA float32 (n, 13); grad: CUDA float32 (16384,); loss: CUDA float32 (1,)."""
+        check(lib().lam_guide_loss_grad(self._h, C.c_void_p(records.data_ptr()), records.shape[0], _fbox(box),
+                                        C.c_void_p(grad.data_ptr()), C.c_void_p(loss.data_ptr()),
+                                        _stream_ptr(stream)))
+
+    def train(self, records, steps, box, stream=None):
+        check(lib().lam_guide_train(self._h, C.c_void_p(records.data_ptr()), records.shape[0], steps, _fbox(box),
+                                    _stream_ptr(stream)))
+
+    def progress(self):
+        st, spp = C.c_uint64(), C.c_uint32()
+        check(lib().lam_guide_progress(self._h, C.byref(st), C.byref(spp)))
+        return st.value, spp.value
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.lam_guide_destroy(self._h)
+            self._h = None

@@ -289,6 +289,15 @@ extern "C" int lam_scene_create(const lam_scene_desc* d, void* stream, lam_scene
     s->stats.blas_node_count = total_nodes;
     s->stats.tlas_node_count = tlas.nodes.size();
     s->stats.build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    for (int k = 0; k < 3; ++k) {
+        s->bounds[k] = ni ? INFINITY : 0.0f;
+        s->bounds[3 + k] = ni ? -INFINITY : 0.0f;
+    }
+    for (uint32_t i = 0; i < ni; ++i)
+        for (int k = 0; k < 3; ++k) {
+            s->bounds[k] = std::min(s->bounds[k], iboxes[6 * i + k]);
+            s->bounds[3 + k] = std::max(s->bounds[3 + k], iboxes[6 * i + 3 + k]);
+        }
     *out = s;
     return LAM_OK;
 }
@@ -308,6 +317,12 @@ extern "C" int lam_scene_update_materials(lam_scene* s, const lam_material* m, u
 extern "C" int lam_scene_stats_get(const lam_scene* s, lam_scene_stats* out) {
     if (!s || !out) return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_scene_stats_get: null argument");
     *out = s->stats;
+    return LAM_OK;
+}
+
+extern "C" int lam_scene_bounds(const lam_scene* s, float box[6]) {
+    if (!s || !box) return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_scene_bounds: null argument");
+    std::memcpy(box, s->bounds, sizeof(s->bounds));
     return LAM_OK;
 }
 

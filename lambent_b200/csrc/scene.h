@@ -55,6 +55,7 @@ struct lam_scene {
     lam::DevScene dev{};
     std::vector<void*> allocations;
     lam_scene_stats stats{};
+    float bounds[6] = {0, 0, 0, 0, 0, 0};  // union of the instance world boxes: lo xyz, hi xyz
     uint32_t blas_count = 0, instance_count = 0, material_count = 0;
     uint32_t diffuse_count = 0, emission_count = 0, attribute_count = 0;
     int device = 0;

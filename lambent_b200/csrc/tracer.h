@@ -59,9 +59,34 @@ struct lam_pipeline {
     lam_stage_times prof{};
     uint64_t prof_segments_base = 0;
     uint64_t total_segments = 0;
+    lam_guide* guide = nullptr;  // learned guide (not owned)
+};
+
+// Learned guiding network state (guide_net.cu).
+struct lam_guide {
+    lam_guide_options opts{};
+    int device = 0, sms = 148;
+    uint32_t parts = 1;                 // gradient partial slots (one per SM)
+    float *master = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+    uint16_t* packed = nullptr;         // BF16 weights in the MMA tile layout
+    float *partial = nullptr, *partial_loss = nullptr;
+    uint32_t* err = nullptr;
+    float* records = nullptr;           // render-side training records, record_capacity entries
+    uint64_t steps = 0;
+    uint32_t trained_spp = 0;
+    bool kernels_ready = false;
+    std::vector<void*> allocs;
 };
 
 namespace lam {
+// Render-side training record: pos, normal, wo, wi, weight (the public lam_guide_record), then the
+// path throughput and accumulated colour at the vertex, and the previous record of the same path.
+constexpr uint32_t GUIDE_RECORD_STRIDE = 20;
+int guide_grad_and_update(lam_guide* g, const float* recs, uint32_t stride, uint32_t n, const uint32_t* n_dev,
+                          uint32_t batch, bool sequential, float scale, const float box[6], uint32_t mode, float* grad,
+                          float* loss, cudaStream_t st);
+int guide_check_error(const lam_guide* g);
+
 int set_intersection_handler(lam_tracer* t, const char* src);
 // Debug views (FrontFace / Reflectance / Tangent), debug.cu.
 int render_debug(lam_pipeline* pl, const lam_scene* s, const lam_camera* cam, const lam_frame_targets* tg,

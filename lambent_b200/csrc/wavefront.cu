@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "guide.cuh"
+#include "guide_net.cuh"
 #include "materials.cuh"
 #include "scene.h"
 #include "tracer.h"
@@ -22,6 +23,7 @@
 namespace lam {
 
 constexpr int WAVE_BLOCK = 128;
+constexpr uint32_t NO_REC = 0xFFFFFFFFu;
 
 struct Isect {
     v3 color;
@@ -165,9 +167,15 @@ struct WaveBuffers {
     // per pixel
     float4 *pix_color = nullptr, *pix_orad = nullptr, *pix_emission = nullptr, *pix_albedo = nullptr;
     lam_markov_chain *tent_snap = nullptr, *tent_live = nullptr;
-    uint32_t* ctr = nullptr;  // [0..1] queue counts, [2..3] work counters, [4] error flags
+    // learned guiding: deferred diffuse vertices and the per-path training-record lists
+    bool learned = false;
+    uint32_t* dq = nullptr;
+    float4 *def_n = nullptr, *def_t = nullptr, *def_c = nullptr;
+    uint32_t* rec_head = nullptr;
+    uint32_t* ctr = nullptr;  // [0..1] queue counts, [2..3] work counters, [4] error flags,
+                              // [8..11] segment counters, [12] diffuse-queue count, [13] records
     std::vector<void*> allocs;
-    int sms = 148, grid_extend = 0, grid_shade = 0;
+    int sms = 148, grid_extend = 0, grid_shade = 0, grid_guide = 0;
 };
 
 static void free_wave(WaveBuffers* w) {
@@ -219,6 +227,15 @@ struct Args {
     // outputs
     float4 *out_color, *out_normal, *out_albedo;
     v3 camera_pos;
+    // learned guiding
+    uint32_t *dq, *dq_count;
+    float4 *def_n, *def_t, *def_c;
+    float* recs;             // training records (GUIDE_RECORD_STRIDE floats), null when not training
+    uint32_t rec_cap;
+    uint32_t *rec_count, *rec_head;
+    const uint16_t* guide_w; // packed BF16 weights
+    float guide_frac;
+    float box[6];
 };
 
 LAM_DEV void create_ray(const Args& A, uint32_t x, uint32_t y, v3* o, v3* d) {
@@ -293,6 +310,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK) generate_kernel(Args A) {
             A.lnormal[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             A.ldir[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
+        if (A.rec_head) A.rec_head[path] = NO_REC;
         A.q_in[path] = path;
         st = rand_u32(st);
     }
@@ -387,7 +405,24 @@ LAM_DEV void screen_candidates(const Args& A, uint32_t pixel, uint32_t fill_seed
     }
 }
 
-template <int Q, bool GUIDE>
+// Learned guiding: colour-weighted luminance of the radiance a path carried back to each recorded
+// vertex, (scol_final - scol_vertex) / throughput_vertex, written as the record's training weight.
+LAM_DEV void finalize_records(const Args& A, uint32_t path, v3 scol) {
+    uint32_t r = A.rec_head[path];
+    for (int guard = 0; r != NO_REC && guard < 256; ++guard) {
+        float* R = A.recs + (size_t)r * GUIDE_RECORD_STRIDE;
+        const float c[3] = {scol.x - R[16], scol.y - R[17], scol.z - R[18]};
+        const float lw[3] = {0.2126f, 0.7152f, 0.0722f};
+        float w = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (R[13 + k] > 0.0f && c[k] > 0.0f) w += lw[k] * (c[k] / R[13 + k]);
+        R[12] = (w < 3.0e38f) ? w : 0.0f;
+        r = __float_as_uint(R[19]);
+    }
+}
+
+template <int Q, bool GUIDE, bool LEARN>
 __global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(Args A) {
     const uint32_t n = *A.count_in;
     const uint32_t lane = threadIdx.x & 31u;
@@ -400,7 +435,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(Args A) {
     for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;; base += gridDim.x * blockDim.x) {
         if (base >= n) break;
         const uint32_t i = base + lane;
-        bool cont = false;
+        bool cont = false, deferred = false;
         uint32_t path = 0;
         if (i < n) {
             path = A.q_in[i];
@@ -541,7 +576,14 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(Args A) {
                 }
                 const bool reflecting = should_reflect || is.ty == TY_METALLIC;
                 if (!reflecting) {
-                    if (is.ty == TY_DIFFUSE) {
+                    if (LEARN && is.ty == TY_DIFFUSE && depth + 1u < A.max_depth) {
+                        // the guide kernel draws the direction; it uses the seeds of the cosine branch
+                        deferred = true;
+                        A.def_n[path] = make_float4(is.normal.x, is.normal.y, is.normal.z, is.roughness.x);
+                        A.def_t[path] = make_float4(is.tangent.x, is.tangent.y, is.tangent.z, __uint_as_float(seed));
+                        A.def_c[path] = make_float4(is.color.x, is.color.y, is.color.z, 0.0f);
+                        seed += 3u;
+                    } else if (is.ty == TY_DIFFUSE) {
                         v3 dir_cos = cosine_hemisphere(seed, is.normal, is.tangent);
                         float cos_pdf = fmaxf(dot(dir_cos, is.normal) / PI_F, 0.0f);
                         float theta = rand_f32(seed) * TAU_F;
@@ -654,9 +696,10 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(Args A) {
                 grid_store(G, spt, snm, start_dir, st);
                 grid_add_radiance(G, spt, snm, start_dir, orad);
             }
+            if (LEARN && terminated && A.rec_head) finalize_records(A, path, scol);
             // write back
             A.acc[path] = make_float4(scol.x, scol.y, scol.z, cached_pdf);
-            if (cont) {
+            if (cont || deferred) {
                 A.thr[path] = make_float4(color.x, color.y, color.z, picked);
                 A.brdf[path] = cached_brdf;
                 A.seed[path] = seed;
@@ -676,14 +719,158 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(Args A) {
                 mc_store(A.tent_live + pixel, tentative);
             }
         }
-        // warp-aggregated append of the surviving paths
-        const uint32_t mask = __ballot_sync(0xFFFFFFFFu, cont);
+        // warp-aggregated append of the surviving paths (deferred ones go to the guide kernel's queue)
+        const bool next = cont && !deferred;
+        const uint32_t mask = __ballot_sync(0xFFFFFFFFu, next);
         if (mask) {
             uint32_t slot = 0;
             if (lane == 0) slot = atomicAdd(A.count_out, __popc(mask));
             slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
-            if (cont) A.q_out[slot + __popc(mask & ((1u << lane) - 1u))] = path;
+            if (next) A.q_out[slot + __popc(mask & ((1u << lane) - 1u))] = path;
         }
+        if (LEARN) {
+            const uint32_t dmask = __ballot_sync(0xFFFFFFFFu, deferred);
+            if (dmask) {
+                uint32_t slot = 0;
+                if (lane == 0) slot = atomicAdd(A.dq_count, __popc(dmask));
+                slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+                if (deferred) A.dq[slot + __popc(dmask & ((1u << lane) - 1u))] = path;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- learned guiding: deferred diffuse sampling
+// One-sample MIS of the cosine lobe (probability 1 - f) and the network's vMF mixture (probability f):
+// pdf(w) = (1 - f) cos/pi + f q(w).  With NET false (untrained network, f = 0) this is the plain cosine
+// branch of the shade kernel, with the same seeds and the same arithmetic.
+constexpr uint32_t GUIDE_SMEM = net::LAYERS * net::LAYER_BYTES + net::X_BYTES + 64u + 128u;
+
+template <int Q, bool NET>
+LAM_DEV void guide_finish(const Args& A, uint32_t path, const net::Lobes* L, bool& out) {
+    const float4 o4 = A.ray_o[path], d4 = A.ray_d[path], dn = A.def_n[path], dt = A.def_t[path], dc = A.def_c[path];
+    const float4 th = A.thr[path], ac = A.acc[path];
+    const v3 ro = mk(o4.x, o4.y, o4.z), rd = mk(d4.x, d4.y, d4.z), n = mk(dn.x, dn.y, dn.z), t = mk(dt.x, dt.y, dt.z);
+    const uint32_t seed0 = __float_as_uint(dt.w);
+    v3 color = mk(th.x, th.y, th.z);
+    const v3 dir_cos = cosine_hemisphere(seed0, n, t);
+    v3 dir = dir_cos;
+    float pdf = fmaxf(dot(dir_cos, n) / PI_F, 0.0f);
+    if (NET) {
+        const float f = A.guide_frac;
+        uint32_t h = rand_u32(seed0 ^ 0x68E31DA4u);
+        const float u = rand_f32(h);
+        if (u < f) {
+            h = rand_u32(h);
+            const float u0 = rand_f32(h);
+            h = rand_u32(h);
+            const float u1 = rand_f32(h);
+            h = rand_u32(h);
+            const float u2 = rand_f32(h);
+            dir = net::mixture_sample(*L, u0, u1, u2);
+        }
+        pdf = (1.0f - f) * fmaxf(dot(dir, n) / PI_F, 0.0f) + f * net::mixture_pdf(*L, dir);
+    }
+    const v3 diffuse = Shader<Q, false>::make_diffuse(mk(dc.x, dc.y, dc.z), rd, n, t, dn.w, dir);
+    const float cached_brdf = fmaxf(dot(dir, n) / PI_F, 0.0f);
+    const float nf = fabsf(cached_brdf) / fmaxf(pdf, 0.001f);
+    const v3 color_pre = color;
+    color = (color * nf) * diffuse;
+    A.thr[path] = make_float4(color.x, color.y, color.z, th.w);
+    A.brdf[path] = cached_brdf;
+    A.acc[path] = make_float4(ac.x, ac.y, ac.z, pdf);
+    A.ray_d[path] = make_float4(dir.x, dir.y, dir.z, 0.0f);
+    if (A.recs) {
+        const uint32_t r = atomicAdd(A.rec_count, 1u);
+        if (r < A.rec_cap) {
+            float* R = A.recs + (size_t)r * GUIDE_RECORD_STRIDE;
+            const float v[GUIDE_RECORD_STRIDE] = {ro.x, ro.y, ro.z, n.x, n.y, n.z, -rd.x, -rd.y, -rd.z, dir.x,
+                                                  dir.y, dir.z, 0.0f, color_pre.x, color_pre.y, color_pre.z,
+                                                  ac.x, ac.y, ac.z, __uint_as_float(A.rec_head[path])};
+#pragma unroll
+            for (uint32_t k = 0; k < GUIDE_RECORD_STRIDE; ++k) R[k] = v[k];
+            A.rec_head[path] = r;
+        }
+    }
+    out = true;
+}
+
+template <int Q, bool NET>
+__global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
+    const uint32_t n = *A.dq_count;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (!NET) {
+        for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < n; base += gridDim.x * blockDim.x) {
+            const uint32_t i = base + lane;
+            bool go = false;
+            uint32_t path = 0;
+            if (i < n) {
+                path = A.dq[i];
+                guide_finish<Q, false>(A, path, nullptr, go);
+            }
+            const uint32_t mask = __ballot_sync(0xFFFFFFFFu, go);
+            uint32_t slot = 0;
+            if (lane == 0 && mask) slot = atomicAdd(A.count_out, __popc(mask));
+            slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+            if (go) A.q_out[slot + __popc(mask & ((1u << lane) - 1u))] = path;
+        }
+        return;
+    }
+    // tensor-core path: 128 deferred vertices per tile, one per thread
+    extern __shared__ uint8_t smraw[];
+    uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smraw) + 127u) & ~uintptr_t(127));
+    uint8_t* W = sm;
+    uint8_t* X = sm + net::LAYERS * net::LAYER_BYTES;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(X + net::X_BYTES);
+    uint32_t* slot_t = reinterpret_cast<uint32_t*>(X + net::X_BYTES + 8);
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(A.guide_w);
+        uint4* dst = reinterpret_cast<uint4*>(W);
+        for (uint32_t i = threadIdx.x; i < net::LAYERS * net::LAYER_BYTES / 16u; i += blockDim.x) dst[i] = src[i];
+    }
+    if (threadIdx.x == 0) net::mbar_init(bar);
+    if (threadIdx.x < 32) net::tmem_alloc(slot_t, 64);
+    net::fence_before();
+    __syncthreads();
+    net::fence_after();
+    net::TileCtx c{*slot_t, net::smem_u32(bar), 0u, false};
+    const uint32_t w_addr = net::smem_u32(W);
+    const uint32_t tiles = (n + net::TILE - 1) / net::TILE;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t i = tile * net::TILE + threadIdx.x;
+        const bool valid = i < n;
+        const uint32_t path = valid ? A.dq[i] : 0u;
+        net::Query q{mk(0.0f, 0.0f, 0.0f), mk(0.0f, 1.0f, 0.0f), mk(0.0f, 1.0f, 0.0f)};
+        if (valid) {
+            const float4 o4 = A.ray_o[path], d4 = A.ray_d[path], dn = A.def_n[path];
+            q.pos = mk(o4.x, o4.y, o4.z);
+            q.n = mk(dn.x, dn.y, dn.z);
+            q.wo = mk(-d4.x, -d4.y, -d4.z);
+        }
+        float f[net::WIDTH];
+        net::encode_features(q, A.box, f);
+        net::store_row(X, net::X_RG, threadIdx.x, f);
+        float raw[net::OUT];
+        if (!net::forward_infer(c, X, w_addr, raw)) break;
+        bool go = false;
+        if (valid) {
+            net::Lobes L;
+            net::lobes_from_raw(raw, L);
+            guide_finish<Q, true>(A, path, &L, go);
+        }
+        const uint32_t mask = __ballot_sync(0xFFFFFFFFu, go);
+        uint32_t slot = 0;
+        if (lane == 0 && mask) slot = atomicAdd(A.count_out, __popc(mask));
+        slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+        if (go) A.q_out[slot + __popc(mask & ((1u << lane) - 1u))] = path;
+    }
+    if (c.failed) net::mbar_wait(c.bar, c.phase ^ 1u);
+    net::fence_before();
+    c.failed = __syncthreads_or(c.failed ? 1 : 0) != 0;
+    if (c.failed && threadIdx.x == 0) atomicOr(A.err, 1u << 8);
+    if (threadIdx.x < 32) {
+        net::fence_after();
+        net::tmem_free(c.tmem, 64);
     }
 }
 
@@ -797,7 +984,7 @@ __global__ void shuffle_kernel(Args A) {
     mc_store(A.tent_snap + p, t);
 }
 
-static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool full, bool guide) {
+static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool full, bool guide, bool learned) {
     const uint32_t npix = width * height;
     uint32_t spp_wave = 1;
     if (!guide && pl->opts.restir_temporal != LAM_RESTIR_PER_SAMPLE) {
@@ -806,7 +993,8 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
         spp_wave = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(pl->opts.samples, target / std::max(1u, npix)));
     }
     WaveBuffers* w = pl->wave;
-    if (w && w->width == width && w->height == height && w->spp_wave == spp_wave && w->full == full && w->guide == guide)
+    if (w && w->width == width && w->height == height && w->spp_wave == spp_wave && w->full == full && w->guide == guide &&
+        w->learned == learned)
         return LAM_OK;
     free_wave(w);
     pl->wave = nullptr;
@@ -818,6 +1006,7 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
     w->paths = (uint64_t)npix * spp_wave;
     w->full = full;
     w->guide = guide;
+    w->learned = learned;
     const size_t P = w->paths;
     int rc = 0;
     rc |= walloc(w, &w->ray_o, P);
@@ -849,6 +1038,13 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
         rc |= walloc(w, &w->tent_snap, npix);
         rc |= walloc(w, &w->tent_live, npix);
     }
+    if (learned) {
+        rc |= walloc(w, &w->dq, P);
+        rc |= walloc(w, &w->def_n, P);
+        rc |= walloc(w, &w->def_t, P);
+        rc |= walloc(w, &w->def_c, P);
+        rc |= walloc(w, &w->rec_head, P);
+    }
     if (rc) {
         free_wave(w);
         return LAM_ERR_CUDA;
@@ -861,16 +1057,32 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, extend_kernel<false>, WAVE_BLOCK, 0);
     w->grid_extend = w->sms * std::max(1, occ);
     occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_kernel<LAM_QUALITY_MEDIUM, false>, WAVE_BLOCK, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_kernel<LAM_QUALITY_MEDIUM, false, false>, WAVE_BLOCK, 0);
     w->grid_shade = w->sms * std::max(1, occ);
+    if (learned) {
+        cudaFuncSetAttribute(guide_sample_kernel<LAM_QUALITY_LOW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, GUIDE_SMEM);
+        cudaFuncSetAttribute(guide_sample_kernel<LAM_QUALITY_MEDIUM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, GUIDE_SMEM);
+        cudaFuncSetAttribute(guide_sample_kernel<LAM_QUALITY_HIGH, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, GUIDE_SMEM);
+        occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, guide_sample_kernel<LAM_QUALITY_MEDIUM, true>, WAVE_BLOCK, GUIDE_SMEM);
+        // at most 4 resident CTAs per SM keep the 64-column TMEM allocations within the 512 columns
+        w->grid_guide = w->sms * std::min(4, std::max(1, occ));
+    }
     pl->wave = w;
     return LAM_OK;
 }
 
 template <int Q>
-static void launch_shade(bool guide, dim3 g, dim3 b, cudaStream_t st, const Args& A) {
-    if (guide) shade_kernel<Q, true><<<g, b, 0, st>>>(A);
-    else shade_kernel<Q, false><<<g, b, 0, st>>>(A);
+static void launch_guide(bool net, int grid, cudaStream_t st, const Args& A) {
+    if (net) guide_sample_kernel<Q, true><<<grid, WAVE_BLOCK, GUIDE_SMEM, st>>>(A);
+    else guide_sample_kernel<Q, false><<<grid, WAVE_BLOCK, 0, st>>>(A);
+}
+
+template <int Q>
+static void launch_shade(bool guide, bool learned, dim3 g, dim3 b, cudaStream_t st, const Args& A) {
+    if (guide) shade_kernel<Q, true, false><<<g, b, 0, st>>>(A);
+    else if (learned) shade_kernel<Q, false, true><<<g, b, 0, st>>>(A);
+    else shade_kernel<Q, false, false><<<g, b, 0, st>>>(A);
 }
 
 }  // namespace lam
@@ -884,7 +1096,6 @@ extern "C" int lam_tracer_create_pipeline(const lam_tracer* t, const lam_pipelin
     if (o->max_depth == 0 || o->max_depth > 255) return set_error(LAM_ERR_INVALID_ARGUMENT, "max_depth must be in 1..255");
     if (o->restir_temporal > LAM_RESTIR_PER_PIXEL) return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown ReSTIR mode");
     if (o->guide_mode > LAM_GUIDE_LEARNED) return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown guide mode");
-    if (o->guide_mode == LAM_GUIDE_LEARNED) return set_error(LAM_ERR_UNSUPPORTED, "learned guiding is not available in this pipeline");
     if (t->quality > LAM_QUALITY_HIGH && (t->quality < LAM_DEBUG_FRONT_FACE || t->quality > LAM_DEBUG_TANGENT))
         return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown shader");
     lam_pipeline* p = new lam_pipeline();
@@ -909,6 +1120,12 @@ extern "C" int lam_pipeline_destroy(lam_pipeline* p) {
     return LAM_OK;
 }
 
+extern "C" int lam_pipeline_set_guide(lam_pipeline* p, lam_guide* g) {
+    if (!p) return set_error(LAM_ERR_INVALID_ARGUMENT, "null pipeline");
+    p->guide = g;
+    return LAM_OK;
+}
+
 extern "C" int lam_pipeline_set_profiling(lam_pipeline* p, int enabled) {
     if (!p) return set_error(LAM_ERR_INVALID_ARGUMENT, "null pipeline");
     p->profiling = enabled != 0;
@@ -926,6 +1143,7 @@ extern "C" int lam_render_profile_get(lam_pipeline* p, lam_stage_times* out) {
             case 0: p->prof.generate_ms += ms; break;
             case 1: p->prof.extend_ms += ms; p->prof.extend_launches++; break;
             case 2: p->prof.shade_ms += ms; p->prof.shade_launches++; break;
+            case 4: p->prof.train_ms += ms; break;
             default: p->prof.accumulate_ms += ms; break;
         }
         p->event_pool.push_back(t.start);
@@ -984,9 +1202,13 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         return set_error(LAM_ERR_LAYOUT_MISMATCH, "scene bindings exceed the pipeline layout counts");
     if (pl->quality >= LAM_DEBUG_FRONT_FACE) return render_debug(pl, s, cam, tg, (cudaStream_t)stream);
     const bool guide = pl->opts.guide_mode == LAM_GUIDE_MARKOV;
+    const bool learned = pl->opts.guide_mode == LAM_GUIDE_LEARNED;
     const uint32_t restir = pl->opts.restir_temporal;
+    if (learned && !pl->guide) return set_error(LAM_ERR_INVALID_ARGUMENT, "LAM_GUIDE_LEARNED needs lam_pipeline_set_guide");
+    if (learned && restir != LAM_RESTIR_DISABLED)
+        return set_error(LAM_ERR_UNSUPPORTED, "learned guiding runs with ReSTIR disabled");
     const bool full = guide || restir != LAM_RESTIR_DISABLED;
-    int rc = ensure_wave(pl, tg->width, tg->height, full, guide);
+    int rc = ensure_wave(pl, tg->width, tg->height, full, guide, learned);
     if (rc) return rc;
     WaveBuffers* w = pl->wave;
     cudaStream_t st = (cudaStream_t)stream;
@@ -1044,6 +1266,18 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
     A.out_normal = (float4*)tg->normal;
     A.out_albedo = (float4*)tg->albedo;
     A.camera_pos = v3{cam->view_inverse[12], cam->view_inverse[13], cam->view_inverse[14]};
+    lam_guide* gd = learned ? pl->guide : nullptr;
+    if (gd) {
+        A.dq = w->dq;
+        A.dq_count = w->ctr + 12;
+        A.def_n = w->def_n;
+        A.def_t = w->def_t;
+        A.def_c = w->def_c;
+        A.rec_cap = gd->opts.record_capacity;
+        A.rec_count = w->ctr + 13;
+        A.guide_w = gd->packed;
+        std::memcpy(A.box, s->bounds, sizeof(A.box));
+    }
     if (guide && !world) return set_error(LAM_ERR_INVALID_ARGUMENT, "Markov guiding needs MARKOV_CHAIN_WORLD_SPACE buffers");
     const bool alpha = !s->dev.all_opaque;
     const dim3 blk(WAVE_BLOCK);
@@ -1080,6 +1314,14 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         uint32_t* cb = w->ctr + 1;
         A.q_in = qa;
         A.count_in = ca;
+        // learned guiding: record training vertices while the guide has seen fewer than train_spp
+        // samples per pixel; sample the network once it has taken a training step
+        const bool training = gd && gd->records && gd->trained_spp < gd->opts.train_spp;
+        const bool use_net = gd && gd->steps > 0;
+        A.recs = training ? gd->records : nullptr;
+        A.rec_head = training ? w->rec_head : nullptr;
+        A.guide_frac = use_net ? gd->opts.guide_fraction : 0.0f;
+        if (training) cudaMemsetAsync(w->ctr + 13, 0, sizeof(uint32_t), st);
         int h = begin(0);
         generate_kernel<<<gpix, blk, 0, st>>>(A);
         end(h);
@@ -1097,13 +1339,23 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
             else extend_kernel<false><<<w->grid_extend, blk, 0, st>>>(A);
             end(h);
             h = begin(2);
+            if (gd) cudaMemsetAsync(w->ctr + 12, 0, sizeof(uint32_t), st);
             switch (pl->quality) {
-                case LAM_QUALITY_LOW: launch_shade<LAM_QUALITY_LOW>(guide, w->grid_shade, blk, st, A); break;
-                case LAM_QUALITY_HIGH: launch_shade<LAM_QUALITY_HIGH>(guide, w->grid_shade, blk, st, A); break;
-                default: launch_shade<LAM_QUALITY_MEDIUM>(guide, w->grid_shade, blk, st, A); break;
+                case LAM_QUALITY_LOW: launch_shade<LAM_QUALITY_LOW>(guide, learned, w->grid_shade, blk, st, A); break;
+                case LAM_QUALITY_HIGH: launch_shade<LAM_QUALITY_HIGH>(guide, learned, w->grid_shade, blk, st, A); break;
+                default: launch_shade<LAM_QUALITY_MEDIUM>(guide, learned, w->grid_shade, blk, st, A); break;
+            }
+            launches += 2;
+            if (gd) {
+                const int gg = use_net ? w->grid_guide : w->grid_shade;
+                switch (pl->quality) {
+                    case LAM_QUALITY_LOW: launch_guide<LAM_QUALITY_LOW>(use_net, gg, st, A); break;
+                    case LAM_QUALITY_HIGH: launch_guide<LAM_QUALITY_HIGH>(use_net, gg, st, A); break;
+                    default: launch_guide<LAM_QUALITY_MEDIUM>(use_net, gg, st, A); break;
+                }
+                ++launches;
             }
             end(h);
-            launches += 2;
             std::swap(qa, qb);
             std::swap(ca, cb);
         }
@@ -1116,6 +1368,18 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         accumulate_kernel<0><<<gpix, blk, 0, st>>>(A, last);
         end(h);
         ++launches;
+        if (training) {
+            h = begin(4);
+            for (uint32_t k = 0; k < gd->opts.steps_per_wave; ++k) {
+                rc = guide_grad_and_update(gd, gd->records, GUIDE_RECORD_STRIDE, gd->opts.record_capacity, w->ctr + 13,
+                                           gd->opts.batch, false, 1.0f / (float)gd->opts.batch, s->bounds, 1u, nullptr,
+                                           nullptr, st);
+                if (rc) return rc;
+                launches += 2;
+            }
+            end(h);
+            gd->trained_spp += A.wave_count;
+        }
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_error(e, "lam_render launch");

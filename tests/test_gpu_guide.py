@@ -1,0 +1,178 @@
+"""Learned path guiding on the B200: the tcgen05 evaluation and training kernels against the CPU
+oracle (oracle/oracle_guide.py), training progress, and the guided renderer (bit-exact fallback
+before training, unbiased and lower-error after it)."""
+import numpy as np
+import pytest
+
+import lambent_b200 as lb
+from lambent_b200 import _abi, scenes
+from oracle import oracle_guide as og
+
+pytestmark = pytest.mark.gpu
+BOX = [-1.0, -1.0, -1.0, 1.0, 1.0, 1.0]
+
+
+def _unit(v):
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def _records(n, seed, vmf_target=False):
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(-1, 1, (n, 3))
+    nrm = _unit(rng.normal(size=(n, 3)))
+    wo = _unit(rng.normal(size=(n, 3)))
+    if vmf_target:
+        # incident directions concentrated (kappa = 20) around a mean that depends on the position
+        mean = _unit(np.stack([np.sin(2 * pos[:, 0]), np.ones(n), np.cos(2 * pos[:, 2])], axis=1))
+        wi = _sample_vmf(rng, mean, 20.0)
+        w = np.ones(n)
+    else:
+        wi = _unit(rng.normal(size=(n, 3)))
+        w = rng.exponential(1.0, n)
+        w[::5] = 0.0
+    return np.concatenate([pos, nrm, wo, wi, w[:, None]], axis=1).astype(np.float32)
+
+
+def _sample_vmf(rng, mean, kappa):
+    n = mean.shape[0]
+    u = rng.uniform(size=n)
+    c = 1.0 + np.log(u + (1 - u) * np.exp(-2 * kappa)) / kappa
+    phi = rng.uniform(0, 2 * np.pi, n)
+    s = np.sqrt(np.maximum(0, 1 - c * c))
+    a = np.where(np.abs(mean[:, :1]) > 0.9, [[0, 1, 0]], [[1, 0, 0]])
+    b1 = _unit(np.cross(mean, a))
+    b2 = np.cross(mean, b1)
+    return _unit(mean * c[:, None] + b1 * (s * np.cos(phi))[:, None] + b2 * (s * np.sin(phi))[:, None])
+
+
+def _guide(**kw):
+    kw.setdefault("record_capacity", 0)
+    return lb.Guide(lb.GuideOptions(**kw))
+
+
+def test_eval_matches_oracle(cuda):
+    import torch
+    g = _guide()
+    params = og.init_params(11)
+    g.set_params(params)
+    n = 1000  # ragged last tile
+    rec = _records(n, 12)
+    q = torch.tensor(rec[:, :9], device="cuda")
+    out = torch.zeros((n, 40), dtype=torch.float32, device="cuda")
+    g.eval(q, BOX, out)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().astype(np.float64)
+    ref, _ = og.forward(params, og.encode(rec[:, 0:3], rec[:, 3:6], rec[:, 6:9], BOX), use_bf16=True)
+    rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    assert rel < 1e-2, rel
+    assert np.max(np.abs(got - ref)) < 5e-2 * np.max(np.abs(ref))
+    assert g.progress() == (0, 0)
+
+
+def test_loss_and_gradient_match_oracle(cuda):
+    import torch
+    g = _guide()
+    params = og.init_params(21)
+    g.set_params(params)
+    n = 1000
+    rec = _records(n, 22)
+    r = torch.tensor(rec, device="cuda")
+    grad = torch.zeros(16384, dtype=torch.float32, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    g.loss_grad(r, BOX, grad, loss)
+    torch.cuda.synchronize()
+    ref_loss, ref_grad = og.loss_and_grad(params, rec.astype(np.float64), BOX, use_bf16=True)
+    assert float(loss.item()) == pytest.approx(ref_loss, rel=2e-3)
+    got = grad.cpu().numpy().astype(np.float64)
+    rel = np.linalg.norm(got - ref_grad) / np.linalg.norm(ref_grad)
+    assert rel < 3e-2, rel
+    # per layer, including the bias columns
+    for l in range(4):
+        a, b = got[l * 4096:(l + 1) * 4096], ref_grad[l * 4096:(l + 1) * 4096]
+        assert np.linalg.norm(a - b) <= 5e-2 * np.linalg.norm(b) + 1e-9, l
+    assert np.all(got[~og.trainable_mask().reshape(-1)] == 0.0)
+
+
+def test_training_fits_a_directional_distribution(cuda):
+    import torch
+    g = _guide(batch=4096, learning_rate=3e-3, seed=5)
+    rec = _records(1 << 16, 31, vmf_target=True)
+    r = torch.tensor(rec, device="cuda")
+    held = torch.tensor(_records(4096, 32, vmf_target=True), device="cuda")
+    grad = torch.zeros(16384, dtype=torch.float32, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    g.loss_grad(held, BOX, grad, loss)
+    torch.cuda.synchronize()
+    before = float(loss.item())
+    g.train(r, 600, BOX)
+    g.loss_grad(held, BOX, grad, loss)
+    torch.cuda.synchronize()
+    after = float(loss.item())
+    assert g.progress()[0] == 600
+    # -E log q: 2.53 for the uniform sphere, about -0.16 for the exact kappa = 20 target
+    assert before > 2.0, before
+    assert after < 0.8, (before, after)
+
+
+def _render(s, samples, guide_mode=_abi.GUIDE_NONE, guide=None, seed=0, depth=5, pipe=None, gscene=None):
+    import torch
+    if pipe is None:
+        tracer = lb.RayTracer(lb.path_tracing.Medium)
+        opts = lb.PathTracerOpts(samples=samples, restir_temporal=_abi.RESTIR_DISABLED, max_depth=depth,
+                                 guide_mode=guide_mode)
+        pipe = tracer.create_pipeline(*s.layout_counts(), opts)
+        if guide is not None:
+            pipe.set_guide(guide)
+    gs = gscene or lb.GpuScene(s)
+    W, H = s.width, s.height
+    bufs = lb.DataBuffers(W, H, 1, 0)
+    col = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
+    pipe.render(gs, bufs, s.camera, lb.targets_from(col), seed)
+    torch.cuda.synchronize()
+    assert pipe.stats().error_flags == 0
+    return col.cpu().numpy()[..., :3].astype(np.float64), pipe, gs
+
+
+def test_untrained_guide_is_the_plain_estimator(cuda):
+    """Before its first training step the learned mode samples the cosine lobe with the plain seeds."""
+    s = scenes.occluded_cornell(64, 64)
+    plain, _, _ = _render(s, 16)
+    g = _guide(train_spp=0)
+    learned, _, _ = _render(s, 16, _abi.GUIDE_LEARNED, g)
+    assert np.array_equal(plain, learned)
+    assert g.progress() == (0, 0)
+
+
+def _block_means(img, b=16):
+    H, W, _ = img.shape
+    return img.reshape(H // b, b, W // b, b, 3).mean(axis=(1, 3))
+
+
+def test_trained_guide_is_unbiased_and_reduces_error(cuda):
+    s = scenes.occluded_cornell(64, 64)
+    g = _guide(train_spp=64, record_capacity=1 << 20, batch=8192, steps_per_wave=200, seed=3)
+    # training render: records the first 64 spp (one wave at this size) and trains after it
+    _, gpipe, gs = _render(s, 64, _abi.GUIDE_LEARNED, g, seed=1000)
+    steps, spp = g.progress()
+    assert steps == 200 and spp == 64
+    reps, spp = 8, 64
+    guided = [_render(s, spp, seed=2000 + k, pipe=gpipe, gscene=gs)[0] for k in range(reps)]
+    assert g.progress()[0] == 200  # no further training
+    ppipe = None
+    plain = []
+    for k in range(reps):
+        img, ppipe, _ = _render(s, spp, seed=3000 + k, pipe=ppipe, gscene=gs)
+        plain.append(img)
+    ref = sum(_render(s, 1024, seed=5000 + k, pipe=ppipe, gscene=gs)[0] for k in range(8)) / 8.0
+    gb = np.stack([_block_means(x) for x in guided])
+    pb = np.stack([_block_means(x) for x in plain])
+    se = np.sqrt(gb.var(axis=0, ddof=1) / reps + pb.var(axis=0, ddof=1) / reps) + 1e-6
+    z = np.abs(gb.mean(axis=0) - pb.mean(axis=0)) / se
+    assert np.all(z < 4.5), z.max()
+
+    def relmse(x):
+        return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    e_guided = np.mean([relmse(x) for x in guided])
+    e_plain = np.mean([relmse(x) for x in plain])
+    assert e_guided < e_plain, (e_guided, e_plain)
