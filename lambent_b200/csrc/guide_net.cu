@@ -201,21 +201,21 @@ __global__ void __launch_bounds__(128, 1) guide_grad_kernel(GradArgs A) {
                 break;
             }
             if (l > 0) {
+                float v[64];
+                tmem_ld64(t_row, v);
 #pragma unroll
-                for (uint32_t c16 = 0; c16 < 4; ++c16) {
-                    float v[16];
-                    tmem_ld16(t_row + 16u * c16, v);
-                    const uint4 x0 = load_chunk(Xs[l], X_RG, row, 2 * c16), x1 = load_chunk(Xs[l], X_RG, row, 2 * c16 + 1);
-                    const uint32_t xw[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+                for (uint32_t ch = 0; ch < 8; ++ch) {
+                    const uint4 x = load_chunk(Xs[l], X_RG, row, ch);
+                    const uint32_t xw[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        if (!(bf16_lo(xw[k]) > 0.0f)) v[2 * k] = 0.0f;
-                        if (!(bf16_hi(xw[k]) > 0.0f)) v[2 * k + 1] = 0.0f;
+                    for (int k = 0; k < 4; ++k) {
+                        if (!(bf16_lo(xw[k]) > 0.0f)) v[8 * ch + 2 * k] = 0.0f;
+                        if (!(bf16_hi(xw[k]) > 0.0f)) v[8 * ch + 2 * k + 1] = 0.0f;
                     }
-                    if (c16 == 3) v[15] = 0.0f;
-                    store_chunk(G, G_RG, row, 2 * c16, v);
-                    store_chunk(G, G_RG, row, 2 * c16 + 1, v + 8);
                 }
+                v[63] = 0.0f;
+#pragma unroll
+                for (uint32_t ch = 0; ch < 8; ++ch) store_chunk(G, G_RG, row, ch, v + 8 * ch);
             }
         }
         any = true;
@@ -233,12 +233,13 @@ __global__ void __launch_bounds__(128, 1) guide_grad_kernel(GradArgs A) {
     if (threadIdx.x < 64) {
         const uint32_t o = threadIdx.x;
         for (uint32_t l = 0; l < 4u; ++l) {
-            for (uint32_t c16 = 0; c16 < 4; ++c16) {
-                float v[16];
-                tmem_ld16(t_row + 64u * (l + 1u) + 16u * c16, v);
-                const bool use = any && !c.failed && trainable(l, o);
-                for (int k = 0; k < 16; ++k) part[l * 4096u + o * 64u + 16u * c16 + k] = use ? v[k] : 0.0f;
-            }
+            float v[64];
+            tmem_ld64(t_row + 64u * (l + 1u), v);
+            const bool use = any && !c.failed && trainable(l, o);
+            float4* dst = reinterpret_cast<float4*>(part + l * 4096u + o * 64u);
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                dst[k] = use ? make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
     }
     if (threadIdx.x == 0) {

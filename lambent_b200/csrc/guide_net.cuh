@@ -128,6 +128,44 @@ LAM_DEV void tmem_ld16(uint32_t taddr, float* v) {
 #pragma unroll
     for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
 }
+// 64 consecutive columns in one load and one wait.
+LAM_DEV void tmem_ld64(uint32_t taddr, float* v) {
+    uint32_t r[64];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, "
+        "%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, "
+        "%48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]),
+          "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]),
+          "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]),
+          "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]),
+          "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        : "r"(taddr));
+#pragma unroll
+    for (int k = 0; k < 64; ++k) v[k] = __uint_as_float(r[k]);
+}
+// 32 + 8 columns (the head) in one statement and one wait.
+LAM_DEV void tmem_ld40(uint32_t taddr, float* v) {
+    uint32_t r[40];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%40];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%32, %33, %34, %35, %36, %37, %38, %39}, [%41];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]),
+          "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39])
+        : "r"(taddr), "r"(taddr + 32u));
+#pragma unroll
+    for (int k = 0; k < 40; ++k) v[k] = __uint_as_float(r[k]);
+}
 LAM_DEV void tmem_ld8(uint32_t taddr, float* v) {
     uint32_t r[8];
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n\t"
@@ -167,29 +205,27 @@ LAM_DEV void encode_features(const Query& q, const float* box, float* f) {
         const float ext = box[3 + a] - box[a];
         float u = ext > 0.0f ? (pc[a] - box[a]) / ext : 0.5f;
         u = fminf(fmaxf(u, 0.0f), 1.0f);
-        float s = u;
+        float sv, cv;
+        sincospif(u, &sv, &cv);
 #pragma unroll
         for (int k = 0; k < 5; ++k) {
-            float sv, cv;
-            sincospif(s, &sv, &cv);
             f[6 * k + 2 * a] = sv;
             f[6 * k + 2 * a + 1] = cv;
-            s = s * 2.0f;
+            const float s2 = 2.0f * sv * cv, c2 = fmaf(-2.0f * sv, sv, 1.0f);  // next octave by angle doubling
+            sv = s2;
+            cv = c2;
         }
     }
     const float d[6] = {q.n.x, q.n.y, q.n.z, q.wo.x, q.wo.y, q.wo.z};
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
         f[30 + c] = d[c];
-        float s = d[c];
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            float sv, cv;
-            sincospif(s, &sv, &cv);
-            f[36 + 4 * c + 2 * k] = sv;
-            f[36 + 4 * c + 2 * k + 1] = cv;
-            s = s * 2.0f;
-        }
+        float sv, cv;
+        sincospif(d[c], &sv, &cv);
+        f[36 + 4 * c] = sv;
+        f[36 + 4 * c + 1] = cv;
+        f[36 + 4 * c + 2] = 2.0f * sv * cv;
+        f[36 + 4 * c + 3] = fmaf(-2.0f * sv, sv, 1.0f);
     }
     f[60] = 0.0f;
     f[61] = 0.0f;
@@ -200,6 +236,7 @@ LAM_DEV void encode_features(const Query& q, const float* box, float* f) {
 // ---------------------------------------------------------------- lobe mixture
 struct Lobes {
     float pi[LOBES], kappa[LOBES];
+    float lognorm[LOBES];  // log(kappa / (2 pi (1 - e^{-2 kappa}))) - kappa
     v3 mu[LOBES];
 };
 LAM_DEV float clampf_(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
@@ -218,7 +255,9 @@ LAM_DEV void lobes_from_raw(const float* raw, Lobes& L) {
 #pragma unroll
     for (int j = 0; j < LOBES; ++j) {
         L.pi[j] *= inv;
-        L.kappa[j] = __expf(clampf_(raw[8 + j], KAPPA_LOG_MIN, KAPPA_LOG_MAX));
+        const float lk = clampf_(raw[8 + j], KAPPA_LOG_MIN, KAPPA_LOG_MAX);
+        L.kappa[j] = __expf(lk);
+        L.lognorm[j] = lk - 1.8378770664093453f - log1pf(-__expf(-2.0f * L.kappa[j])) - L.kappa[j];
         v3 m = mk(raw[16 + j], raw[24 + j], raw[32 + j]);
         const float l = len(m);
         L.mu[j] = l > 1e-12f ? m / l : mk(0.0f, 1.0f, 0.0f);
@@ -233,7 +272,7 @@ LAM_DEV float vmf_log_pdf(float kappa, float cos_mu) {
 LAM_DEV float mixture_pdf(const Lobes& L, v3 w) {
     float p = 0.0f;
 #pragma unroll
-    for (int j = 0; j < LOBES; ++j) p += L.pi[j] * __expf(vmf_log_pdf(L.kappa[j], dot(L.mu[j], w)));
+    for (int j = 0; j < LOBES; ++j) p += L.pi[j] * __expf(fmaf(L.kappa[j], dot(L.mu[j], w), L.lognorm[j]));
     return p;
 }
 
@@ -366,22 +405,15 @@ LAM_DEV void store_row(uint8_t* tile, uint32_t rg, uint32_t row, const float* f)
 
 // Hidden-layer epilogue: ReLU of this thread's accumulator row into `dst`; column 63 is the constant 1.
 LAM_DEV void epilogue_relu(uint32_t t_row, uint8_t* dst, uint32_t row) {
+    float v[64];
+    tmem_ld64(t_row, v);
 #pragma unroll
-    for (uint32_t c16 = 0; c16 < 4; ++c16) {
-        float v[16];
-        tmem_ld16(t_row + 16u * c16, v);
+    for (int k = 0; k < 64; ++k) v[k] = fmaxf(v[k], 0.0f);
+    v[63] = 1.0f;
 #pragma unroll
-        for (int k = 0; k < 16; ++k) v[k] = fmaxf(v[k], 0.0f);
-        if (c16 == 3) v[15] = 1.0f;
-        store_chunk(dst, X_RG, row, 2 * c16, v);
-        store_chunk(dst, X_RG, row, 2 * c16 + 1, v + 8);
-    }
+    for (uint32_t c = 0; c < 8; ++c) store_chunk(dst, X_RG, row, c, v + 8 * c);
 }
-LAM_DEV void head_read(uint32_t t_row, float* raw) {
-    tmem_ld16(t_row, raw);
-    tmem_ld16(t_row + 16u, raw + 16);
-    tmem_ld8(t_row + 32u, raw + 32);
-}
+LAM_DEV void head_read(uint32_t t_row, float* raw) { tmem_ld40(t_row, raw); }
 
 // Forward pass of a tile whose features are in X (overwritten layer by layer); raw = head outputs.
 LAM_DEV bool forward_infer(TileCtx& c, uint8_t* X, uint32_t w_addr, float* raw) {

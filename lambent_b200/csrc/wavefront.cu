@@ -232,6 +232,7 @@ struct Args {
     float4 *def_n, *def_t, *def_c;
     float* recs;             // training records (GUIDE_RECORD_STRIDE floats), null when not training
     uint32_t rec_cap;
+    float rec_prob;          // probability that a deferred vertex is recorded
     uint32_t *rec_count, *rec_head;
     const uint16_t* guide_w; // packed BF16 weights
     float guide_frac;
@@ -744,7 +745,8 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(Args A) {
 // One-sample MIS of the cosine lobe (probability 1 - f) and the network's vMF mixture (probability f):
 // pdf(w) = (1 - f) cos/pi + f q(w).  With NET false (untrained network, f = 0) this is the plain cosine
 // branch of the shade kernel, with the same seeds and the same arithmetic.
-constexpr uint32_t GUIDE_SMEM = net::LAYERS * net::LAYER_BYTES + net::X_BYTES + 64u + 128u;
+constexpr uint32_t GUIDE_SMEM = net::LAYERS * net::LAYER_BYTES + 2u * net::X_BYTES + 64u + 128u;
+constexpr uint32_t GUIDE_TMEM_COLS = 128;  // accumulators of tiles A (columns 0..63) and B (64..127)
 
 template <int Q, bool NET>
 LAM_DEV void guide_finish(const Args& A, uint32_t path, const net::Lobes* L, bool& out) {
@@ -780,7 +782,9 @@ LAM_DEV void guide_finish(const Args& A, uint32_t path, const net::Lobes* L, boo
     A.brdf[path] = cached_brdf;
     A.acc[path] = make_float4(ac.x, ac.y, ac.z, pdf);
     A.ray_d[path] = make_float4(dir.x, dir.y, dir.z, 0.0f);
-    if (A.recs) {
+    // a Bernoulli subset of the vertices (probability rec_prob), so that the record buffer samples every
+    // pixel and depth of the wave instead of filling up with the first vertices shaded
+    if (A.recs && rand_f32(rand_u32(seed0 ^ 0x2C1B3C6Du)) < A.rec_prob) {
         const uint32_t r = atomicAdd(A.rec_count, 1u);
         if (r < A.rec_cap) {
             float* R = A.recs + (size_t)r * GUIDE_RECORD_STRIDE;
@@ -816,61 +820,112 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
         }
         return;
     }
-    // tensor-core path: 128 deferred vertices per tile, one per thread
+    // tensor-core path: two 128-row tiles (A, B) per pass, one row of each per thread, so that tile B's
+    // MMAs run while tile A's epilogue does and both tiles' gathers are in flight together
     extern __shared__ uint8_t smraw[];
     uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smraw) + 127u) & ~uintptr_t(127));
     uint8_t* W = sm;
-    uint8_t* X = sm + net::LAYERS * net::LAYER_BYTES;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(X + net::X_BYTES);
-    uint32_t* slot_t = reinterpret_cast<uint32_t*>(X + net::X_BYTES + 8);
+    uint8_t* XA = sm + net::LAYERS * net::LAYER_BYTES;
+    uint8_t* XB = XA + net::X_BYTES;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(XB + net::X_BYTES);
+    uint32_t* slot_t = reinterpret_cast<uint32_t*>(bars + 2);
     {
         const uint4* src = reinterpret_cast<const uint4*>(A.guide_w);
         uint4* dst = reinterpret_cast<uint4*>(W);
         for (uint32_t i = threadIdx.x; i < net::LAYERS * net::LAYER_BYTES / 16u; i += blockDim.x) dst[i] = src[i];
     }
-    if (threadIdx.x == 0) net::mbar_init(bar);
-    if (threadIdx.x < 32) net::tmem_alloc(slot_t, 64);
+    if (threadIdx.x == 0) {
+        net::mbar_init(bars);
+        net::mbar_init(bars + 1);
+    }
+    if (threadIdx.x < 32) net::tmem_alloc(slot_t, GUIDE_TMEM_COLS);
     net::fence_before();
     __syncthreads();
     net::fence_after();
-    net::TileCtx c{*slot_t, net::smem_u32(bar), 0u, false};
-    const uint32_t w_addr = net::smem_u32(W);
-    const uint32_t tiles = (n + net::TILE - 1) / net::TILE;
-    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const uint32_t i = tile * net::TILE + threadIdx.x;
-        const bool valid = i < n;
-        const uint32_t path = valid ? A.dq[i] : 0u;
-        net::Query q{mk(0.0f, 0.0f, 0.0f), mk(0.0f, 1.0f, 0.0f), mk(0.0f, 1.0f, 0.0f)};
-        if (valid) {
-            const float4 o4 = A.ray_o[path], d4 = A.ray_d[path], dn = A.def_n[path];
-            q.pos = mk(o4.x, o4.y, o4.z);
-            q.n = mk(dn.x, dn.y, dn.z);
-            q.wo = mk(-d4.x, -d4.y, -d4.z);
+    const uint32_t tmem = *slot_t;
+    const uint32_t bar_a = net::smem_u32(bars), bar_b = net::smem_u32(bars + 1);
+    const uint32_t w_addr = net::smem_u32(W), xa = net::smem_u32(XA), xb = net::smem_u32(XB);
+    const uint32_t t_row = tmem + ((threadIdx.x & ~31u) << 16);
+    uint32_t phase = 0;
+    bool failed = false;
+    const uint32_t pairs = (n + 2u * net::TILE - 1) / (2u * net::TILE);
+    for (uint32_t pair = blockIdx.x; pair < pairs; pair += gridDim.x) {
+        const uint32_t ia = pair * 2u * net::TILE + threadIdx.x, ib = ia + net::TILE;
+        const bool va = ia < n, vb = ib < n;
+        const uint32_t pa = va ? A.dq[ia] : 0u, pb = vb ? A.dq[ib] : 0u;
+        auto query = [&](bool v, uint32_t path, uint8_t* X) {
+            net::Query q{mk(0.0f, 0.0f, 0.0f), mk(0.0f, 1.0f, 0.0f), mk(0.0f, 1.0f, 0.0f)};
+            if (v) {
+                const float4 o4 = A.ray_o[path], d4 = A.ray_d[path], dn = A.def_n[path];
+                q.pos = mk(o4.x, o4.y, o4.z);
+                q.n = mk(dn.x, dn.y, dn.z);
+                q.wo = mk(-d4.x, -d4.y, -d4.z);
+                // the sampling epilogue reads these after the network: start them toward L2 now
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.def_t + path));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.def_c + path));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.thr + path));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.acc + path));
+            }
+            float f[net::WIDTH];
+            net::encode_features(q, A.box, f);
+            net::store_row(X, net::X_RG, threadIdx.x, f);
+        };
+        query(va, pa, XA);
+        query(vb, pb, XB);
+        bool ok = true;
+        for (uint32_t l = 0; l < (uint32_t)net::LAYERS; ++l) {
+            net::fence_async_smem();
+            net::fence_before();
+            if (__syncthreads_or(failed ? 1 : 0)) {
+                failed = true;
+                ok = false;
+                break;
+            }
+            if (threadIdx.x == 0) {
+                net::fence_after();
+                net::issue_fwd(tmem, xa, w_addr + l * net::LAYER_BYTES);
+                net::mma_commit(bar_a);
+                net::issue_fwd(tmem + 64u, xb, w_addr + l * net::LAYER_BYTES);
+                net::mma_commit(bar_b);
+            }
+            if (!net::mbar_wait(bar_a, phase)) failed = true;
+            net::fence_after();
+            if (l < 3u) net::epilogue_relu(t_row, XA, threadIdx.x);
+            if (!net::mbar_wait(bar_b, phase)) failed = true;
+            net::fence_after();
+            if (l < 3u) net::epilogue_relu(t_row + 64u, XB, threadIdx.x);
+            phase ^= 1u;
         }
-        float f[net::WIDTH];
-        net::encode_features(q, A.box, f);
-        net::store_row(X, net::X_RG, threadIdx.x, f);
-        float raw[net::OUT];
-        if (!net::forward_infer(c, X, w_addr, raw)) break;
-        bool go = false;
-        if (valid) {
-            net::Lobes L;
-            net::lobes_from_raw(raw, L);
-            guide_finish<Q, true>(A, path, &L, go);
+        if (!ok) break;
+        for (uint32_t h = 0; h < 2u; ++h) {
+            const bool v = h == 0u ? va : vb;
+            const uint32_t path = h == 0u ? pa : pb;
+            float raw[net::OUT];
+            net::head_read(t_row + 64u * h, raw);
+            bool go = false;
+            if (v) {
+                net::Lobes L;
+                net::lobes_from_raw(raw, L);
+                guide_finish<Q, true>(A, path, &L, go);
+            }
+            const uint32_t mask = __ballot_sync(0xFFFFFFFFu, go);
+            uint32_t slot = 0;
+            if (lane == 0 && mask) slot = atomicAdd(A.count_out, __popc(mask));
+            slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+            if (go) A.q_out[slot + __popc(mask & ((1u << lane) - 1u))] = path;
         }
-        const uint32_t mask = __ballot_sync(0xFFFFFFFFu, go);
-        uint32_t slot = 0;
-        if (lane == 0 && mask) slot = atomicAdd(A.count_out, __popc(mask));
-        slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
-        if (go) A.q_out[slot + __popc(mask & ((1u << lane) - 1u))] = path;
     }
-    if (c.failed) net::mbar_wait(c.bar, c.phase ^ 1u);
+    if (failed) {
+        // let MMAs still in flight finish before TMEM is freed
+        net::mbar_wait(bar_a, phase ^ 1u);
+        net::mbar_wait(bar_b, phase ^ 1u);
+    }
     net::fence_before();
-    c.failed = __syncthreads_or(c.failed ? 1 : 0) != 0;
-    if (c.failed && threadIdx.x == 0) atomicOr(A.err, 1u << 8);
+    failed = __syncthreads_or(failed ? 1 : 0) != 0;
+    if (failed && threadIdx.x == 0) atomicOr(A.err, 1u << 8);
     if (threadIdx.x < 32) {
         net::fence_after();
-        net::tmem_free(c.tmem, 64);
+        net::tmem_free(tmem, GUIDE_TMEM_COLS);
     }
 }
 
@@ -1060,13 +1115,31 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_kernel<LAM_QUALITY_MEDIUM, false, false>, WAVE_BLOCK, 0);
     w->grid_shade = w->sms * std::max(1, occ);
     if (learned) {
-        cudaFuncSetAttribute(guide_sample_kernel<LAM_QUALITY_LOW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, GUIDE_SMEM);
-        cudaFuncSetAttribute(guide_sample_kernel<LAM_QUALITY_MEDIUM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, GUIDE_SMEM);
-        cudaFuncSetAttribute(guide_sample_kernel<LAM_QUALITY_HIGH, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, GUIDE_SMEM);
-        occ = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, guide_sample_kernel<LAM_QUALITY_MEDIUM, true>, WAVE_BLOCK, GUIDE_SMEM);
-        // at most 4 resident CTAs per SM keep the 64-column TMEM allocations within the 512 columns
-        w->grid_guide = w->sms * std::min(4, std::max(1, occ));
+        cudaError_t e = cudaSuccess;
+        auto attrs = [&](const void* k) {
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, GUIDE_SMEM);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+        };
+        attrs((const void*)guide_sample_kernel<LAM_QUALITY_LOW, true>);
+        attrs((const void*)guide_sample_kernel<LAM_QUALITY_MEDIUM, true>);
+        attrs((const void*)guide_sample_kernel<LAM_QUALITY_HIGH, true>);
+        // resident CTAs per SM from the kernel's registers and shared memory (the occupancy query
+        // under-reports this kernel); at most 4 keep the 128-column TMEM allocations within 512 columns
+        cudaFuncAttributes fa{};
+        int regs_sm = 0, smem_sm = 0, smem_reserved = 0;
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void*)guide_sample_kernel<LAM_QUALITY_MEDIUM, true>);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, pl->device);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, pl->device);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_reserved, cudaDevAttrReservedSharedMemoryPerBlock, pl->device);
+        if (e != cudaSuccess) {
+            free_wave(w);
+            return cuda_error(e, "guide kernel attributes");
+        }
+        const int regs_block = ((fa.numRegs + 7) / 8) * 8 * WAVE_BLOCK;
+        const int by_regs = regs_block > 0 ? regs_sm / regs_block : 1;
+        const int by_smem = smem_sm / (int)(GUIDE_SMEM + fa.sharedSizeBytes + smem_reserved);
+        w->grid_guide = w->sms * std::min(4, std::max(1, std::min(by_regs, by_smem)));
     }
     pl->wave = w;
     return LAM_OK;
@@ -1319,6 +1392,11 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         const bool training = gd && gd->records && gd->trained_spp < gd->opts.train_spp;
         const bool use_net = gd && gd->steps > 0;
         A.recs = training ? gd->records : nullptr;
+        if (training) {
+            // expected diffuse vertices of the wave: at most one per path and bounce
+            const double expected = (double)w->npix * A.wave_count * std::max(1u, pl->opts.max_depth - 1u);
+            A.rec_prob = (float)std::min(1.0, 1.25 * gd->opts.record_capacity / std::max(1.0, expected));
+        }
         A.rec_head = training ? w->rec_head : nullptr;
         A.guide_frac = use_net ? gd->opts.guide_fraction : 0.0f;
         if (training) cudaMemsetAsync(w->ctr + 13, 0, sizeof(uint32_t), st);
