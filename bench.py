@@ -1,5 +1,6 @@
 #!/usr/bin/env python
-"""Benchmark of the plain wavefront path tracer at scale (Mrays/s at 1080p / 1.31M triangles).
+"""Benchmark of the wavefront path tracer: Mrays/s at 1080p / 1.31M triangles (plain), and the
+equal-time relMSE of the learned-guided renderer against the plain one (the "guided" object).
 
 Workload (one GPU): seeded displaced-icosphere field, 64 instances x 20,480 triangles (1.31M f32
 triangles), 16-layer 1024^2 value-noise textures, 1920x1080, Medium shader, depth 12, no guiding,
@@ -44,6 +45,14 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--out", default=None, help="also write the JSON line to this file")
+    p.add_argument("--no-guided", action="store_true", help="skip the guided-vs-plain equal-time measurement")
+    p.add_argument("--guided-width", type=int, default=1920)
+    p.add_argument("--guided-height", type=int, default=1080)
+    p.add_argument("--guided-ref-spp", type=int, default=16384, help="spp of the plain reference image")
+    p.add_argument("--guided-depth", type=int, default=8)
+    p.add_argument("--guided-frac", type=float, default=0.5)
+    p.add_argument("--guided-train-spp", type=int, default=32)
+    p.add_argument("--guided-steps-per-wave", type=int, default=25)
     return p.parse_args()
 
 
@@ -192,6 +201,127 @@ def emit(line, a):
             f.write(s + "\n")
 
 
+def guided_equal_time(a, dev):
+    """Equal-time relMSE of the learned-guided renderer against the plain one.
+
+    Scene: the procedural Cornell box with a single 0.2 x 0.2 emitter above an occluding plate
+    (indirect-heavy lighting), Medium shader, ReSTIR off.  The plain form renders 1024 spp in time T.
+    The guided form (a fresh network, trained online on its first `train_spp` samples) renders
+    32-spp chunks; its running mean is compared with the reference after each chunk, outside the
+    timed region.  relMSE = mean((x - ref)^2 / (ref^2 + 1e-2)) against a plain reference of
+    `ref_spp` samples; the reference's own noise, estimated from its two halves, is subtracted.
+    """
+    import torch
+    import lambent_b200 as lb
+    from lambent_b200 import _abi, scenes
+    W, H = a.guided_width, a.guided_height
+    s = scenes.occluded_cornell(W, H)
+    gs = lb.GpuScene(s)
+    bufs = lb.DataBuffers(W, H, 1, 0)
+    col = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
+    tg = lb.targets_from(col)
+    stream = torch.cuda.current_stream()
+
+    def pipe(samples, mode=_abi.GUIDE_NONE, guide=None):
+        p = lb.RayTracer(lb.path_tracing.Medium).create_pipeline(*s.layout_counts(), lb.PathTracerOpts(
+            samples=samples, restir_temporal=_abi.RESTIR_DISABLED, max_depth=a.guided_depth, guide_mode=mode))
+        if guide is not None:
+            p.set_guide(guide)
+        return p
+
+    def timed(p, seed):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        p.render(gs, bufs, s.camera, tg, seed, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    # reference: two independent halves
+    pr = pipe(1024)
+    halves = []
+    t_ref = time.perf_counter()
+    for h in range(2):
+        acc = torch.zeros((H, W, 3), dtype=torch.float64, device=dev)
+        n = max(1, a.guided_ref_spp // 2048)
+        for k in range(n):
+            pr.render(gs, bufs, s.camera, tg, 1_000_000 + (h * n + k) * 1024, stream)
+            acc += col[..., :3].double()
+        halves.append(acc / n)
+    torch.cuda.synchronize()
+    t_ref = time.perf_counter() - t_ref
+    ref = (halves[0] + halves[1]) / 2
+    den = ref ** 2 + 1e-2
+    ref_noise = float((((halves[0] - halves[1]) ** 2) / den).mean()) / 4.0
+
+    def relmse(img):
+        return float((((img.double() - ref) ** 2) / den).mean()) - ref_noise
+
+    # plain: 1024 spp in one call (after a warm-up call)
+    p1 = pipe(1024)
+    timed(p1, 5)
+    T = min(timed(p1, 77 + 8191 * r) for r in range(2))
+    e_plain = relmse(col[..., :3])
+    segs_plain = p1.stats().ray_segments
+    # guided: fresh network, 32-spp chunks until 1024 spp or 1.1 T
+    g = lb.Guide(lb.GuideOptions(train_spp=a.guided_train_spp, steps_per_wave=a.guided_steps_per_wave,
+                                 guide_fraction=a.guided_frac, learning_rate=5e-3, seed=1))
+    pg = pipe(32, _abi.GUIDE_LEARNED, g)
+    acc = torch.zeros((H, W, 3), dtype=torch.float64, device=dev)
+    t, curve, k = 0.0, [], 0
+    while k < 32 and (t < 1.1 * T or k < 2):
+        t += timed(pg, 424242 + 32 * k)
+        acc += col[..., :3].double()
+        k += 1
+        curve.append([32 * k, round(t, 5), relmse(acc / k)])
+    assert pg.stats().error_flags == 0, "guided render reported an error"
+
+    def time_to(target):
+        prev = None
+        for spp, tt, e in curve:
+            if e <= target:
+                if prev is None:
+                    return tt
+                (t0, e0) = prev
+                # interpolate in log relMSE (relMSE ~ 1/time)
+                import math
+                f = (math.log(e0) - math.log(target)) / max(1e-12, math.log(e0) - math.log(e))
+                return t0 + f * (tt - t0)
+            prev = (tt, e)
+        return None
+
+    def at_time(T_):
+        import math
+        prev = None
+        for spp, tt, e in curve:
+            if tt >= T_:
+                if prev is None:
+                    return e
+                t0, e0 = prev
+                f = (T_ - t0) / max(1e-12, tt - t0)
+                return math.exp(math.log(e0) + f * (math.log(e) - math.log(e0)))
+            prev = (tt, e)
+        return None
+
+    t_hit = time_to(e_plain)
+    e_eq = at_time(T)
+    steps, trained = g.progress()
+    return {
+        "config": {"workload": f"occluded-light Cornell box (0.2x0.2 emitter above a plate), {W}x{H}, depth "
+                               f"{a.guided_depth}, Medium, ReSTIR off",
+                   "plain_spp": 1024, "reference_spp": 2 * max(1, a.guided_ref_spp // 2048) * 1024,
+                   "network": "4 x 64 MLP, BF16 tcgen05, 8 vMF lobes, one-sample MIS with the cosine lobe",
+                   "guide_fraction": a.guided_frac, "train_spp": a.guided_train_spp,
+                   "adam_steps": steps},
+        "plain": {"time_s": round(T, 5), "relmse": round(e_plain, 6), "mrays_per_s": round(segs_plain / T / 1e6, 1)},
+        "time_to_plain_quality_ratio": None if t_hit is None else round(t_hit / T, 4),
+        "relmse_ratio_at_equal_time": None if e_eq is None else round(e_eq / e_plain, 4),
+        "ref_noise_relmse": round(ref_noise, 7), "reference_seconds": round(t_ref, 2),
+        "guided_curve": [[spp, tt, round(e, 6)] for spp, tt, e in curve],
+        "target": "time_to_plain_quality_ratio <= 0.5 (relMSE of 1024-spp plain reached in half its time)",
+    }
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -327,6 +457,10 @@ def run_ours(a):
         }
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_reference(a, scene, a.cpu_seconds)
+        if not a.no_guided and world == 1:
+            del gscene, pipe, bufs
+            torch.cuda.empty_cache()
+            line["guided"] = guided_equal_time(a, dev)
         emit(line, a)
     if world > 1:
         dist.destroy_process_group()
