@@ -46,6 +46,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--out", default=None, help="also write the JSON line to this file")
     p.add_argument("--no-guided", action="store_true", help="skip the guided-vs-plain equal-time measurement")
+    p.add_argument("--guided-only", action="store_true", help="run only the guided-vs-plain measurement")
     p.add_argument("--guided-width", type=int, default=1920)
     p.add_argument("--guided-height", type=int, default=1080)
     p.add_argument("--guided-ref-spp", type=int, default=16384, help="spp of the plain reference image")
@@ -470,6 +471,10 @@ def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.guided_only:
+        import torch
+        torch.cuda.set_device(0)
+        emit({"metric": "equal-time relMSE guided vs plain", "guided": guided_equal_time(a, torch.device("cuda", 0))}, a)
     else:
         run_ours(a)
 
