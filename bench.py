@@ -1,6 +1,7 @@
 #!/usr/bin/env python
-"""Benchmark of the wavefront path tracer: Mrays/s at 1080p / 1.31M triangles (plain), and the
-equal-time relMSE of the learned-guided renderer against the plain one (the "guided" object).
+"""Benchmark of the wavefront path tracer: Mrays/s at 1080p / 1.31M triangles (plain), the
+equal-time relMSE of the learned-guided renderer against the plain one (the "guided" object), and
+batched serving of 64 uneven requests in one CUDA-graph launch (the "batched" object).
 
 Workload (one GPU): seeded displaced-icosphere field, 64 instances x 20,480 triangles (1.31M f32
 triangles), 16-layer 1024^2 value-noise textures, 1920x1080, Medium shader, depth 12, no guiding,
@@ -54,6 +55,10 @@ def parse():
     p.add_argument("--guided-frac", type=float, default=0.5)
     p.add_argument("--guided-train-spp", type=int, default=32)
     p.add_argument("--guided-steps-per-wave", type=int, default=25)
+    p.add_argument("--no-batched", action="store_true", help="skip the batched-serving measurement")
+    p.add_argument("--batched-only", action="store_true", help="run only the batched-serving measurement")
+    p.add_argument("--batched-requests", type=int, default=64)
+    p.add_argument("--batched-scenes", type=int, default=8, help="distinct scenes shared by the requests")
     return p.parse_args()
 
 
@@ -323,6 +328,97 @@ def guided_equal_time(a, dev):
     }
 
 
+def batched_serving(a, dev):
+    """Batched serving-style render: independent requests in one lam_batch_render, replayed as a
+    CUDA graph with the autotuner's queue and launch sizes.
+
+    Requests: resolutions uniform over {256^2, 512^2, 768x432, 1024^2}, spp uniform over {4, 16, 64},
+    scenes from the Cornell-box generator filled with subdivided boxes up to 10k-500k triangles
+    (log-uniform; `batched_scenes` distinct scenes shared by the requests), Medium, depth 8, seeded.
+    Reports aggregate samples/s over the batch, per-request latency from the batch start to the
+    request's completion (p50 / p99), and the same requests rendered one lam_render at a time.
+    """
+    import math
+    import numpy as np
+    import torch
+    import lambent_b200 as lb
+    from lambent_b200 import _abi, scenes
+    rng = np.random.default_rng(2024)
+    tri_counts = [int(round(math.exp(rng.uniform(math.log(10_000), math.log(500_000)))))
+                  for _ in range(a.batched_scenes)]
+    t0 = time.perf_counter()
+    geo = [scenes.box_field(n, 256, 256, seed=k) for k, n in enumerate(tri_counts)]
+    gsc = [lb.GpuScene(s) for s in geo]
+    build_s = time.perf_counter() - t0
+    sizes = [(256, 256), (512, 512), (768, 432), (1024, 1024)]
+    reqs, keep = [], []
+    for k in range(a.batched_requests):
+        w, h = sizes[rng.integers(0, 4)]
+        spp = int([4, 16, 64][rng.integers(0, 3)])
+        sc = int(rng.integers(0, len(geo)))
+        cam = scenes.make_camera((0.0, 1.0, 3.4), (0.0, 1.0, 0.0), 40.0, w / h)
+        col = torch.zeros((h, w, 4), dtype=torch.float32, device=dev)
+        keep.append(col)
+        reqs.append((gsc[sc], cam, lb.targets_from(col), spp, 1000 * k))
+    samples = sum(r[2].width * r[2].height * r[3] for r in reqs)
+    opts = lb.PathTracerOpts(samples=1, restir_temporal=_abi.RESTIR_DISABLED, max_depth=8)
+    pipe = lb.RayTracer(lb.path_tracing.Medium).create_pipeline(8, 8, 8, 8, opts)
+    t0 = time.perf_counter()
+    tuning = pipe.batch_autotune(reqs, spp_divisor=4)
+    tune_s = time.perf_counter() - t0
+    stream = torch.cuda.current_stream()
+    pipe.batch_render(reqs, tuning, stream)  # graph capture + first replay
+    torch.cuda.synchronize()
+    times, lats = [], []
+    for rep in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pipe.batch_render(reqs, tuning, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+        lats.append(pipe.batch_latencies(len(reqs)))
+    best = int(np.argmin(times))
+    T, lat = times[best], np.asarray(lats[best])
+    assert pipe.stats().error_flags == 0
+    segs = pipe.stats().ray_segments
+    # the same requests one lam_render at a time, for comparison
+    singles = {}
+    seq = 0.0
+    seq_done = []  # completion time of each request when rendered one at a time, in submission order
+    for (g, cam, tg, spp, seed) in reqs:
+        key = (spp, tg.width, tg.height)
+        if key not in singles:
+            singles[key] = lb.RayTracer(lb.path_tracing.Medium).create_pipeline(8, 8, 8, 8, lb.PathTracerOpts(
+                samples=spp, restir_temporal=_abi.RESTIR_DISABLED, max_depth=8))
+        p1 = singles[key]
+        bufs = lb.DataBuffers(tg.width, tg.height, 1, 0)
+        p1.render(g, bufs, cam, tg, seed, stream)  # warm-up (buffer allocation)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        p1.render(g, bufs, cam, tg, seed, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        seq += e0.elapsed_time(e1) / 1e3
+        seq_done.append(seq * 1e3)
+    return {
+        "config": {"workload": f"{len(reqs)} requests, resolutions {{256^2, 512^2, 768x432, 1024^2}}, spp {{4, 16, 64}}, "
+                               f"{len(geo)} box-field Cornell scenes of {min(tri_counts)}-{max(tri_counts)} triangles "
+                               "(log-uniform 10k-500k), Medium, depth 8",
+                   "triangles": tri_counts, "samples": int(samples),
+                   "tuning": {"wave_paths": tuning.wave_paths, "extend_blocks_per_sm": tuning.extend_blocks_per_sm,
+                              "shade_blocks_per_sm": tuning.shade_blocks_per_sm, "cuda_graph": bool(tuning.use_graph)},
+                   "autotune_s": round(tune_s, 2), "scene_build_s": round(build_s, 2)},
+        "batch_s": round(T, 4), "samples_per_s": round(samples / T, 1), "mrays_per_s": round(segs / T / 1e6, 1),
+        "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 2), "p99": round(float(np.percentile(lat, 99)), 2),
+                       "max": round(float(lat.max()), 2)},
+        "sequential_s": round(seq, 4), "speedup_vs_sequential": round(seq / T, 3),
+        "sequential_latency_ms": {"p50": round(float(np.percentile(seq_done, 50)), 2),
+                                  "p99": round(float(np.percentile(seq_done, 99)), 2)},
+    }
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -458,10 +554,13 @@ def run_ours(a):
         }
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_reference(a, scene, a.cpu_seconds)
-        if not a.no_guided and world == 1:
+        if world == 1 and not (a.no_guided and a.no_batched):
             del gscene, pipe, bufs
             torch.cuda.empty_cache()
+        if not a.no_guided and world == 1:
             line["guided"] = guided_equal_time(a, dev)
+        if not a.no_batched and world == 1:
+            line["batched"] = batched_serving(a, dev)
         emit(line, a)
     if world > 1:
         dist.destroy_process_group()
@@ -471,6 +570,10 @@ def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.batched_only:
+        import torch
+        torch.cuda.set_device(0)
+        emit({"metric": "batched serving samples/s", "batched": batched_serving(a, torch.device("cuda", 0))}, a)
     elif a.guided_only:
         import torch
         torch.cuda.set_device(0)

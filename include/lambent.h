@@ -430,6 +430,39 @@ int lam_spatial_resampling(lam_data_buffers* buffers, const lam_frame_targets* t
                            uint32_t is_samples, uint32_t is_space, uint32_t seed_offset,
                            void* stream);
 
+/* ---------------------------------------------------------------- batched renders
+ * lam_batch_render: many independent render requests (own scene, camera, resolution and sample
+ * count) as one wavefront.  Paths of every request share the same persistent launches, so small
+ * requests fill the GPU together.  No reference counterpart: the reference dispatches one rt_main
+ * per request.  Plain path tracing only (no ReSTIR, no guiding); each request writes the mean
+ * colour of its samples to targets.color, and normal/albedo of its last sample when given.
+ * Requests run shortest first (pixels x samples) and finish at different times inside the batch:
+ * lam_batch_latencies reports, per request, the time from the batch start to its completion. */
+typedef struct lam_batch_request {
+    const lam_scene* scene;
+    lam_camera camera;
+    lam_frame_targets targets;
+    uint32_t samples;
+    uint32_t seed_offset;
+} lam_batch_request;
+/* Queue and launch sizes of a batch (0 = default).  use_graph: capture the launch sequence in a
+ * CUDA graph on the first call and replay it while the requests (pointers, sizes, samples) and the
+ * tuning stay the same. */
+typedef struct lam_batch_tuning {
+    uint32_t wave_paths;       /* paths per wave (queue size), >= the largest request's pixels */
+    uint32_t extend_blocks_per_sm;
+    uint32_t shade_blocks_per_sm;
+    uint32_t use_graph;
+} lam_batch_tuning;
+int lam_batch_render(lam_pipeline* pipeline, const lam_batch_request* requests, uint32_t n,
+                     const lam_batch_tuning* tuning, void* stream);
+/* Milliseconds from the start of the last batch to each request's completion (synchronises). */
+int lam_batch_latencies(lam_pipeline* pipeline, uint32_t n, double* ms);
+/* Autotuner: times the batch (samples divided by `spp_divisor`, at least 1) under candidate wave
+ * sizes and launch sizes, coordinate by coordinate, and writes the fastest to *out. */
+int lam_batch_autotune(lam_pipeline* pipeline, const lam_batch_request* requests, uint32_t n,
+                       uint32_t spp_divisor, lam_batch_tuning* out, void* stream);
+
 /* ---------------------------------------------------------------- learned path guiding
  * No counterpart in the reference (its guiding is the Markov-chain cache, general.wesl:764-866).
  * A 4-layer MLP (64 wide, BF16 weights, FP32 accumulation on the tensor cores) maps a diffuse

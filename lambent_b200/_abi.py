@@ -129,6 +129,15 @@ class StageTimes(C.Structure):
                 ("ray_segments", u64), ("train_ms", C.c_double)]
 
 
+class BatchRequest(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("camera", Camera), ("targets", FrameTargets), ("samples", u32),
+                ("seed_offset", u32)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("wave_paths", u32), ("extend_blocks_per_sm", u32), ("shade_blocks_per_sm", u32), ("use_graph", u32)]
+
+
 class GuideOptions(C.Structure):
     _fields_ = [("train_spp", u32), ("steps_per_wave", u32), ("batch", u32), ("record_capacity", u32),
                 ("learning_rate", C.c_float), ("guide_fraction", C.c_float), ("seed", u32)]

@@ -101,6 +101,9 @@ def lib():
     _sig(L, "lam_guide_progress", i, vp, P(C.c_uint64), u32p)
     _sig(L, "lam_pipeline_set_guide", i, vp, vp)
     _sig(L, "lam_scene_bounds", i, vp, f32p)
+    _sig(L, "lam_batch_render", i, vp, P(_abi.BatchRequest), u32, P(_abi.BatchTuning), vp)
+    _sig(L, "lam_batch_latencies", i, vp, u32, P(C.c_double))
+    _sig(L, "lam_batch_autotune", i, vp, P(_abi.BatchRequest), u32, u32, P(_abi.BatchTuning), vp)
     _LIB = L
     return L
 
@@ -417,6 +420,31 @@ class Pipeline:
 
     def profile_reset(self):
         check(lib().lam_render_profile_reset(self._h))
+
+    def batch_render(self, requests, tuning=None, stream=None):
+        """requests: list of (GpuScene, Camera, FrameTargets, samples, seed_offset).  Renders all of them as
+        one wavefront (lam_batch_render); tuning: a _abi.BatchTuning or None for the defaults."""
+        arr = self._batch_array(requests)
+        check(lib().lam_batch_render(self._h, arr, len(requests), C.byref(tuning) if tuning is not None else None,
+                                     _stream_ptr(stream)))
+
+    def batch_latencies(self, n):
+        out = (C.c_double * n)()
+        check(lib().lam_batch_latencies(self._h, n, out))
+        return list(out)
+
+    def batch_autotune(self, requests, spp_divisor=4, stream=None):
+        arr = self._batch_array(requests)
+        t = _abi.BatchTuning()
+        check(lib().lam_batch_autotune(self._h, arr, len(requests), spp_divisor, C.byref(t), _stream_ptr(stream)))
+        return t
+
+    def _batch_array(self, requests):
+        arr = (_abi.BatchRequest * len(requests))()
+        for k, (scene, camera, targets, samples, seed) in enumerate(requests):
+            arr[k] = _abi.BatchRequest(scene._h.value, camera.c, targets, samples, seed)
+        self._batch_keep = (arr, requests)
+        return arr
 
     def set_guide(self, guide):
         """Attaches a learned Guide (used when the options' guide_mode is GuideMode.LEARNED)."""

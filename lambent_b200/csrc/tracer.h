@@ -36,6 +36,8 @@ struct lam_data_buffers {
 namespace lam {
 
 struct WaveBuffers;  // defined in wavefront.cu
+struct BatchState;   // defined in wavefront.cu
+void free_batch(BatchState* b);
 
 }  // namespace lam
 
@@ -60,6 +62,8 @@ struct lam_pipeline {
     uint64_t prof_segments_base = 0;
     uint64_t total_segments = 0;
     lam_guide* guide = nullptr;  // learned guide (not owned)
+    lam::BatchState* batch = nullptr;  // lam_batch_render state
+    uint32_t* stats_ctr = nullptr;     // device counters of the last render (single or batched)
 };
 
 // Learned guiding network state (guide_net.cu).

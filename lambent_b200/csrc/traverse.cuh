@@ -383,6 +383,45 @@ LAM_DEV void trace_persistent(const DevScene& S, const uint4* __restrict__ tl, c
     }
 }
 
+// As trace_persistent, for work items that belong to different scenes: `load(i, o, d, t0, t1, sp)`
+// also returns the item's scene, whose TLAS and instances are read from global memory.
+template <bool ANY, bool ALPHA, class Load, class Store>
+LAM_DEV void trace_persistent_multi(uint32_t n, uint32_t* __restrict__ work, uint32_t& err, Load load, Store store) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    Traverser<ANY, ALPHA> T;
+    uint2 stack[TRAVERSAL_STACK];
+    const DevScene* sp = nullptr;
+    bool active = false, exhausted = false;
+    uint32_t item = 0;
+    for (;;) {
+        const uint32_t act = __ballot_sync(0xFFFFFFFFu, active);
+        if (!exhausted && __popc(act) < REFILL_THRESHOLD) {
+            const uint32_t need = ~act;
+            const uint32_t leader = __ffs(need) - 1u;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(work, (uint32_t)__popc(need));
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (!active) {
+                const uint32_t i = base + __popc(need & lt_mask);
+                if (i < n) {
+                    float3 o, d;
+                    float t0, t1;
+                    load(i, o, d, t0, t1, sp);
+                    T.init(*sp, o, d, t0, t1);
+                    item = i;
+                    active = true;
+                }
+            }
+            if (base + (uint32_t)__popc(need) >= n) exhausted = true;
+        }
+        if (!__any_sync(0xFFFFFFFFu, active)) break;
+        if (active && !T.step(*sp, sp->tlas_nodes, sp->inst, stack, err)) {
+            store(item, T.res);
+            active = false;
+        }
+    }
+}
 
 constexpr int TRACE_BLOCK = 128;
 constexpr uint32_t SMEM_TLAS_NODES = 64;   // TLAS staged in shared memory when it fits

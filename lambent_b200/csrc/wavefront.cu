@@ -194,6 +194,23 @@ static int walloc(WaveBuffers* w, T** p, size_t count) {
     return LAM_OK;
 }
 
+// ---------------------------------------------------------------- batched renders
+// A request of lam_batch_render: its scene, camera, image and samples.
+struct BatchReq {
+    DevScene S;
+    lam_camera cam;
+    v3 camera_pos;
+    uint32_t width, height, npix, samples, seed_offset;
+    uint32_t pix_base;  // first entry of this request's pixels in the batch's per-pixel pools
+    float4 *out_color, *out_normal, *out_albedo;
+};
+// A segment of a wave: `count` consecutive samples (from `first`) of every pixel of one request,
+// as paths path_base + s * npix + pixel.
+struct BatchSeg {
+    uint32_t req, first, count, path_base;
+    uint32_t pix_thread_base;  // first generate/accumulate thread of the segment within its wave
+};
+
 // ---------------------------------------------------------------- kernel arguments
 struct Args {
     DevScene S;
@@ -237,6 +254,12 @@ struct Args {
     const uint16_t* guide_w; // packed BF16 weights
     float guide_frac;
     float box[6];
+    // batched renders
+    const BatchReq* reqs;
+    const BatchSeg* segs;    // this wave's segments
+    uint32_t nsegs, pix_threads;
+    uint32_t* req_done;      // per request: pixels finished
+    unsigned long long* req_time;  // per request: global timer at completion; [n] = batch start
 };
 
 LAM_DEV void create_ray(const Args& A, uint32_t x, uint32_t y, v3* o, v3* d) {
@@ -423,8 +446,8 @@ LAM_DEV void finalize_records(const Args& A, uint32_t path, v3 scol) {
     }
 }
 
-template <int Q, bool GUIDE, bool LEARN>
-__global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(Args A) {
+template <int Q, bool GUIDE, bool LEARN, bool BATCH>
+__global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(const __grid_constant__ Args A) {
     const uint32_t n = *A.count_in;
     const uint32_t lane = threadIdx.x & 31u;
     Grid G;
@@ -440,10 +463,27 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(Args A) {
         uint32_t path = 0;
         if (i < n) {
             path = A.q_in[i];
-            const uint32_t pixel = path % A.npix;
-            const uint32_t sample_index = A.wave_first + path / A.npix;
-            const bool last_sample = sample_index + 1u == A.samples;
             uint32_t fl = A.flags[path];
+            // per-render fields; a batched render takes them from the path's request
+            const DevScene* Sp = &A.S;
+            uint32_t pixel, sample_index, samples = A.samples;
+            float4 *out_normal = A.out_normal, *out_albedo = A.out_albedo;
+            if (BATCH) {
+                const BatchSeg sg = A.segs[fl >> 16];
+                const BatchReq& R = A.reqs[sg.req];
+                Sp = &R.S;
+                const uint32_t rel = path - sg.path_base;
+                pixel = rel % R.npix;
+                sample_index = sg.first + rel / R.npix;
+                samples = R.samples;
+                out_normal = R.out_normal;
+                out_albedo = R.out_albedo;
+            } else {
+                pixel = path % A.npix;
+                sample_index = A.wave_first + path / A.npix;
+            }
+            const DevScene& S = *Sp;
+            const bool last_sample = sample_index + 1u == samples;
             const uint32_t depth = fl & 0xFFu;
             bool last_not_vmf = (fl >> 8) & 1u;
             const float4 o4 = A.ray_o[path], d4 = A.ray_d[path];
@@ -477,7 +517,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(Args A) {
             bool terminated = false;
             if (h.x != NO_HIT) {
                 Isect is;
-                make_isect(A.S, A.S.inst, h, make_float3(ro.x, ro.y, ro.z), make_float3(rd.x, rd.y, rd.z), is);
+                make_isect(S, S.inst, h, make_float3(ro.x, ro.y, ro.z), make_float3(rd.x, rd.y, rd.z), is);
                 v3 new_pos = fma3(rd, splat(is.t), ro);
                 if (depth != 0u) {
                     v3 est = GUIDE ? grid_radiance(G, new_pos, is.normal, rd) : splat(0.0f);
@@ -506,8 +546,8 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(Args A) {
                         pn = make_float4(is.normal.x, is.normal.y, is.normal.z, pn.w);
                     }
                     if (last_sample) {
-                        if (A.out_normal) A.out_normal[pixel] = make_float4(is.normal.x, is.normal.y, is.normal.z, 1.0f);
-                        if (A.out_albedo) A.out_albedo[pixel] = make_float4(is.color.x, is.color.y, is.color.z, 1.0f);
+                        if (out_normal) out_normal[pixel] = make_float4(is.normal.x, is.normal.y, is.normal.z, 1.0f);
+                        if (out_albedo) out_albedo[pixel] = make_float4(is.color.x, is.color.y, is.color.z, 1.0f);
                         if (A.pix_emission) {
                             A.pix_emission[pixel] = make_float4(is.emission.x, is.emission.y, is.emission.z, 0.0f);
                             A.pix_albedo[pixel] = make_float4(is.color.x, is.color.y, is.color.z, 0.0f);
@@ -650,15 +690,15 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(Args A) {
                 cont = depth + 1u < A.max_depth;
                 terminated = !cont;
             } else {
-                v3 bg = sky_sample(A.S, rd);
+                v3 bg = sky_sample(S, rd);
                 v3 new_pos = fma3(rd, splat(A.tmax), ro);
                 if (depth == 1u && rec) {
                     A.vpoint[path] = make_float4(new_pos.x, new_pos.y, new_pos.z, 0.0f);
                     A.vnormal[path] = make_float4(-rd.x, -rd.y, -rd.z, 0.0f);
                 }
                 if (depth == 0u && last_sample) {
-                    if (A.out_normal) A.out_normal[pixel] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-                    if (A.out_albedo) A.out_albedo[pixel] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+                    if (out_normal) out_normal[pixel] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+                    if (out_albedo) out_albedo[pixel] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
                     if (A.pix_emission) {
                         A.pix_emission[pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                         A.pix_albedo[pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -704,7 +744,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(Args A) {
                 A.thr[path] = make_float4(color.x, color.y, color.z, picked);
                 A.brdf[path] = cached_brdf;
                 A.seed[path] = seed;
-                A.flags[path] = (depth + 1u) | (last_not_vmf ? 0x100u : 0u);
+                A.flags[path] = (fl & 0xFFFF0000u) | (depth + 1u) | (last_not_vmf ? 0x100u : 0u);
                 A.ray_o[path] = make_float4(ro.x, ro.y, ro.z, 0.0f);
                 A.ray_d[path] = make_float4(rd.x, rd.y, rd.z, 0.0f);
             }
@@ -1112,7 +1152,7 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, extend_kernel<false>, WAVE_BLOCK, 0);
     w->grid_extend = w->sms * std::max(1, occ);
     occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_kernel<LAM_QUALITY_MEDIUM, false, false>, WAVE_BLOCK, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_kernel<LAM_QUALITY_MEDIUM, false, false, false>, WAVE_BLOCK, 0);
     w->grid_shade = w->sms * std::max(1, occ);
     if (learned) {
         cudaError_t e = cudaSuccess;
@@ -1153,11 +1193,137 @@ static void launch_guide(bool net, int grid, cudaStream_t st, const Args& A) {
 
 template <int Q>
 static void launch_shade(bool guide, bool learned, dim3 g, dim3 b, cudaStream_t st, const Args& A) {
-    if (guide) shade_kernel<Q, true, false><<<g, b, 0, st>>>(A);
-    else if (learned) shade_kernel<Q, false, true><<<g, b, 0, st>>>(A);
-    else shade_kernel<Q, false, false><<<g, b, 0, st>>>(A);
+    if (guide) shade_kernel<Q, true, false, false><<<g, b, 0, st>>>(A);
+    else if (learned) shade_kernel<Q, false, true, false><<<g, b, 0, st>>>(A);
+    else shade_kernel<Q, false, false, false><<<g, b, 0, st>>>(A);
 }
 
+
+// ---------------------------------------------------------------- batched renders: kernels
+LAM_DEV uint64_t global_timer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Segment of pixel thread t (segments sorted by pix_thread_base).
+LAM_DEV uint32_t find_seg(const BatchSeg* segs, uint32_t nsegs, uint32_t t) {
+    uint32_t lo = 0, hi = nsegs - 1u;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) >> 1;
+        if (segs[mid].pix_thread_base <= t) lo = mid;
+        else hi = mid - 1u;
+    }
+    return lo;
+}
+
+// create_ray (general.wesl:1158-1173) with a request's camera and image size.
+LAM_DEV void create_ray_req(const BatchReq& R, uint32_t x, uint32_t y, v3* o, v3* d) {
+    float hx = __uint2float_rn(R.width) / 2.0f, hy = __uint2float_rn(R.height) / 2.0f;
+    float nx = (__uint2float_rn(x) / hx) - 1.0f, ny = (__uint2float_rn(y) / hy) - 1.0f;
+    float v[4] = {nx, -ny, 1.0f, 1.0f};
+    const float* P = R.cam.projection_inverse;
+    float q[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q[i] = P[i] * v[0] + P[4 + i] * v[1] + P[8 + i] * v[2] + P[12 + i] * v[3];
+    float l = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q[i] = q[i] / l;
+    const float* V = R.cam.view_inverse;
+    *d = mk(V[0] * q[0] + V[4] * q[1] + V[8] * q[2] + V[12] * 0.0f, V[1] * q[0] + V[5] * q[1] + V[9] * q[2] + V[13] * 0.0f,
+            V[2] * q[0] + V[6] * q[1] + V[10] * q[2] + V[14] * 0.0f);
+    *o = R.camera_pos;
+}
+
+// Zeroes the per-request completion counters and stamps the batch start.
+__global__ void batch_start_kernel(uint32_t* done, unsigned long long* times, uint32_t n) {
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) done[i] = 0u;
+    __syncthreads();
+    if (threadIdx.x == 0) times[n] = global_timer_ns();
+}
+
+// One thread per (segment, pixel): the request's seed chain and camera ray for each of the
+// segment's samples (as generate_kernel does for a single render).
+__global__ void __launch_bounds__(WAVE_BLOCK) batch_generate_kernel(const __grid_constant__ Args A) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) *A.count_in = A.npix;  // paths of this wave
+    if (t >= A.pix_threads) return;
+    const uint32_t k = find_seg(A.segs, A.nsegs, t);
+    const BatchSeg sg = A.segs[k];
+    const BatchReq& R = A.reqs[sg.req];
+    const uint32_t p = t - sg.pix_thread_base;
+    const uint32_t x = p % R.width, y = p / R.width;
+    uint32_t st;
+    if (sg.first == 0u) {
+        st = rand_u32(x * y) + R.seed_offset + y;
+        A.pix_color[R.pix_base + p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    } else {
+        st = A.pixel_seed[R.pix_base + p];
+    }
+    v3 o, d;
+    create_ray_req(R, x, y, &o, &d);
+    for (uint32_t j = 0; j < sg.count; ++j) {
+        const uint32_t path = sg.path_base + j * R.npix + p;
+        st = advance_fill_seed(st);
+        A.seed[path] = st;
+        A.ray_o[path] = make_float4(o.x, o.y, o.z, 0.0f);
+        A.ray_d[path] = make_float4(d.x, d.y, d.z, 0.0f);
+        A.thr[path] = make_float4(1.0f, 1.0f, 1.0f, -1.0f);
+        A.acc[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        A.brdf[path] = 0.0f;
+        A.flags[path] = k << 16;
+        A.q_in[path] = path;
+        st = rand_u32(st);
+    }
+    A.pixel_seed[R.pix_base + p] = st;
+}
+
+template <bool ALPHA>
+__global__ void __launch_bounds__(WAVE_BLOCK) extend_batch_kernel(const __grid_constant__ Args A) {
+    const uint32_t n = *A.count_in;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(A.segments, (unsigned long long)n);
+        atomicAdd(A.segments + 1, (unsigned long long)n);
+    }
+    uint32_t err = 0u;
+    trace_persistent_multi<false, ALPHA>(
+        n, A.work, err,
+        [&](uint32_t i, float3& o, float3& d, float& t0, float& t1, const DevScene*& sp) {
+            const uint32_t path = A.q_in[i];
+            const float4 o4 = A.ray_o[path], d4 = A.ray_d[path];
+            o = make_float3(o4.x, o4.y, o4.z);
+            d = make_float3(d4.x, d4.y, d4.z);
+            t0 = A.tmin;
+            t1 = A.tmax;
+            sp = &A.reqs[A.segs[A.flags[path] >> 16].req].S;
+        },
+        [&](uint32_t i, const TraceResult& tr) { A.hit[A.q_in[i]] = make_uint2(tr.tri, tr.inst); });
+    if (err) atomicOr(A.err, err);
+}
+
+// One thread per (segment, pixel): sums the segment's samples in sample order; after a request's
+// last sample writes its mean colour and, for the last pixel to finish, its completion time.
+__global__ void __launch_bounds__(WAVE_BLOCK) batch_accumulate_kernel(const __grid_constant__ Args A) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= A.pix_threads) return;
+    const BatchSeg sg = A.segs[find_seg(A.segs, A.nsegs, t)];
+    const BatchReq& R = A.reqs[sg.req];
+    const uint32_t p = t - sg.pix_thread_base;
+    const float4 pc = A.pix_color[R.pix_base + p];
+    v3 col = mk(pc.x, pc.y, pc.z);
+    for (uint32_t j = 0; j < sg.count; ++j) {
+        const float4 a = A.acc[sg.path_base + j * R.npix + p];
+        col = col + mk(a.x, a.y, a.z);
+    }
+    A.pix_color[R.pix_base + p] = make_float4(col.x, col.y, col.z, 0.0f);
+    if (sg.first + sg.count != R.samples) return;
+    if (R.out_color) {
+        const v3 c = col / __uint2float_rn(R.samples);
+        R.out_color[p] = make_float4(fmaxf(c.x, 0.0f), fmaxf(c.y, 0.0f), fmaxf(c.z, 0.0f), 1.0f);
+    }
+    __threadfence();
+    if (atomicAdd(A.req_done + sg.req, 1u) + 1u == R.npix) A.req_time[sg.req] = global_timer_ns();
+}
 }  // namespace lam
 
 using namespace lam;
@@ -1184,6 +1350,7 @@ extern "C" int lam_tracer_create_pipeline(const lam_tracer* t, const lam_pipelin
 extern "C" int lam_pipeline_destroy(lam_pipeline* p) {
     if (!p) return LAM_OK;
     free_wave(p->wave);
+    free_batch(p->batch);
     for (auto& t : p->timed) {
         cudaEventDestroy(t.start);
         cudaEventDestroy(t.end);
@@ -1246,9 +1413,9 @@ extern "C" int lam_render_profile_reset(lam_pipeline* p) {
 extern "C" int lam_render_stats_get(const lam_pipeline* p, lam_render_stats* out) {
     if (!p || !out) return set_error(LAM_ERR_INVALID_ARGUMENT, "null argument");
     lam_pipeline* q = const_cast<lam_pipeline*>(p);
-    if (q->stats_pending && q->wave) {
+    if (q->stats_pending && q->stats_ctr) {
         uint32_t host[16];
-        cudaError_t e = cudaMemcpy(host, q->wave->ctr, sizeof(host), cudaMemcpyDeviceToHost);
+        cudaError_t e = cudaMemcpy(host, q->stats_ctr, sizeof(host), cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) return cuda_error(e, "lam_render_stats_get");
         unsigned long long segs, total;
         std::memcpy(&segs, host + 8, sizeof(segs));
@@ -1281,6 +1448,8 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
     if (learned && restir != LAM_RESTIR_DISABLED)
         return set_error(LAM_ERR_UNSUPPORTED, "learned guiding runs with ReSTIR disabled");
     const bool full = guide || restir != LAM_RESTIR_DISABLED;
+    pl->stats_ctr = nullptr;  // the counters may move with the wave buffers
+    pl->stats_pending = false;
     int rc = ensure_wave(pl, tg->width, tg->height, full, guide, learned);
     if (rc) return rc;
     WaveBuffers* w = pl->wave;
@@ -1462,7 +1631,404 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_error(e, "lam_render launch");
     pl->stats.samples = (uint64_t)w->npix * pl->opts.samples;
+    pl->stats_ctr = w->ctr;
     pl->stats.kernel_launches = launches;
     pl->stats_pending = true;
+    return LAM_OK;
+}
+
+// ---------------------------------------------------------------- batched renders: host side
+namespace lam {
+
+struct BatchState {
+    WaveBuffers* wave = nullptr;  // path state for `capacity` paths
+    uint32_t capacity = 0;
+    BatchReq* reqs = nullptr;
+    BatchSeg* segs = nullptr;
+    uint32_t* done = nullptr;
+    unsigned long long* times = nullptr;
+    float4* pix_color = nullptr;
+    uint32_t* pixel_seed = nullptr;
+    size_t reqs_cap = 0, segs_cap = 0, done_cap = 0, times_cap = 0, pix_cap = 0, seed_cap = 0;
+    uint64_t generation = 0;  // bumped whenever a buffer moves (invalidates a captured graph)
+    uint32_t last_n = 0;
+    cudaStream_t stream = nullptr;  // capture stream (the legacy default stream cannot be captured)
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    std::vector<char> graph_key;
+};
+
+void free_batch(BatchState* b) {
+    if (!b) return;
+    free_wave(b->wave);
+    cudaFree(b->reqs);
+    cudaFree(b->segs);
+    cudaFree(b->done);
+    cudaFree(b->times);
+    cudaFree(b->pix_color);
+    cudaFree(b->pixel_seed);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->ev_in) cudaEventDestroy(b->ev_in);
+    if (b->ev_out) cudaEventDestroy(b->ev_out);
+    delete b;
+}
+
+struct BatchPlan {
+    std::vector<BatchSeg> segs;
+    std::vector<uint32_t> wave_begin, wave_nsegs, wave_paths, wave_threads;
+    std::vector<uint32_t> pix_base;
+    size_t pixels = 0;
+};
+
+// Shortest requests first (pixels x samples); each wave takes whole sample planes of requests until
+// `capacity` paths.
+static BatchPlan plan_batch(const lam_batch_request* r, uint32_t n, uint32_t capacity) {
+    BatchPlan P;
+    P.pix_base.resize(n);
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        order[i] = i;
+        P.pix_base[i] = (uint32_t)P.pixels;
+        P.pixels += (size_t)r[i].targets.width * r[i].targets.height;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+        return (uint64_t)r[a].targets.width * r[a].targets.height * r[a].samples <
+               (uint64_t)r[b].targets.width * r[b].targets.height * r[b].samples;
+    });
+    uint32_t used = 0, threads = 0, begin = 0;
+    auto close = [&]() {
+        if (P.segs.size() == begin) return;
+        P.wave_begin.push_back(begin);
+        P.wave_nsegs.push_back((uint32_t)P.segs.size() - begin);
+        P.wave_paths.push_back(used);
+        P.wave_threads.push_back(threads);
+        begin = (uint32_t)P.segs.size();
+        used = threads = 0;
+    };
+    for (uint32_t q : order) {
+        const uint32_t npix = r[q].targets.width * r[q].targets.height;
+        uint32_t first = 0;
+        while (first < r[q].samples) {
+            uint32_t fit = (capacity - used) / npix;
+            if (fit == 0 || P.segs.size() - begin >= 255) {
+                close();
+                fit = capacity / npix;
+            }
+            fit = std::min(fit, r[q].samples - first);
+            BatchSeg sg;
+            sg.req = q;
+            sg.first = first;
+            sg.count = fit;
+            sg.path_base = used;
+            sg.pix_thread_base = threads;
+            P.segs.push_back(sg);
+            used += fit * npix;
+            threads += npix;
+            first += fit;
+        }
+    }
+    close();
+    return P;
+}
+
+template <class T>
+static int dgrow(BatchState* b, T** p, size_t* cap, size_t need) {
+    if (*cap >= need && *p) return LAM_OK;
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    b->generation++;
+    cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(1, need) * sizeof(T));
+    if (e != cudaSuccess) return cuda_error(e, "cudaMalloc (batch)");
+    *cap = need;
+    return LAM_OK;
+}
+
+static int batch_wave_buffers(BatchState* b, uint32_t capacity) {
+    if (b->wave && b->capacity >= capacity) return LAM_OK;
+    b->generation++;
+    free_wave(b->wave);
+    b->wave = nullptr;
+    WaveBuffers* w = new WaveBuffers();
+    w->paths = capacity;
+    int rc = 0;
+    rc |= walloc(w, &w->ray_o, capacity);
+    rc |= walloc(w, &w->ray_d, capacity);
+    rc |= walloc(w, &w->hit, capacity);
+    rc |= walloc(w, &w->queue0, capacity);
+    rc |= walloc(w, &w->queue1, capacity);
+    rc |= walloc(w, &w->thr, capacity);
+    rc |= walloc(w, &w->acc, capacity);
+    rc |= walloc(w, &w->brdf, capacity);
+    rc |= walloc(w, &w->seed, capacity);
+    rc |= walloc(w, &w->flags, capacity);
+    rc |= walloc(w, &w->ctr, 64);
+    if (rc) {
+        free_wave(w);
+        return LAM_ERR_CUDA;
+    }
+    cudaMemset(w->ctr, 0, 64 * sizeof(uint32_t));
+    b->wave = w;
+    b->capacity = capacity;
+    return LAM_OK;
+}
+
+static void batch_key(const lam_batch_request* r, uint32_t n, const lam_batch_tuning& t, uint64_t generation,
+                      std::vector<char>& key) {
+    key.resize(sizeof(uint32_t) + n * sizeof(lam_batch_request) + sizeof(t) + sizeof(generation));
+    char* k = key.data();
+    std::memcpy(k, &n, sizeof(n));
+    std::memcpy(k + sizeof(n), r, n * sizeof(lam_batch_request));
+    std::memcpy(k + sizeof(n) + n * sizeof(lam_batch_request), &t, sizeof(t));
+    std::memcpy(k + sizeof(n) + n * sizeof(lam_batch_request) + sizeof(t), &generation, sizeof(generation));
+}
+
+}  // namespace lam
+
+extern "C" int lam_batch_render(lam_pipeline* pl, const lam_batch_request* reqs, uint32_t n,
+                                const lam_batch_tuning* tuning_in, void* stream) {
+    if (!pl || (n && !reqs)) return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_batch_render: null argument");
+    if (n == 0) return LAM_OK;
+    if (pl->quality >= LAM_DEBUG_FRONT_FACE) return set_error(LAM_ERR_UNSUPPORTED, "batched renders use the path-tracing shaders");
+    if (pl->opts.guide_mode != LAM_GUIDE_NONE || pl->opts.restir_temporal != LAM_RESTIR_DISABLED)
+        return set_error(LAM_ERR_UNSUPPORTED, "batched renders are plain path tracing (no guiding, ReSTIR disabled)");
+    uint32_t max_pix = 0;
+    bool all_opaque = true;
+    for (uint32_t i = 0; i < n; ++i) {
+        const lam_batch_request& r = reqs[i];
+        if (!r.scene || r.samples == 0 || r.targets.width == 0 || r.targets.height == 0)
+            return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_batch_render: request without scene, samples or size");
+        if ((uint64_t)r.targets.width * r.targets.height > (1u << 26))
+            return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_batch_render: request image too large");
+        const lam_scene* sc = r.scene;
+        if (sc->instance_count > pl->layout.blas_count || sc->diffuse_count > pl->layout.diffuse_count ||
+            sc->emission_count > pl->layout.emission_count || sc->attribute_count > pl->layout.attribute_count)
+            return set_error(LAM_ERR_LAYOUT_MISMATCH, "a request's scene exceeds the pipeline layout counts");
+        max_pix = std::max(max_pix, r.targets.width * r.targets.height);
+        all_opaque = all_opaque && sc->dev.all_opaque;
+    }
+    lam_batch_tuning t{};
+    if (tuning_in) t = *tuning_in;
+    if (!t.wave_paths) t.wave_paths = 8u << 20;
+    t.wave_paths = std::max(t.wave_paths, max_pix);
+    if (!pl->batch) pl->batch = new BatchState();
+    BatchState* b = pl->batch;
+    pl->stats_ctr = nullptr;  // the counters may move with the batch buffers
+    pl->stats_pending = false;
+    int rc = batch_wave_buffers(b, t.wave_paths);
+    if (rc) return rc;
+    WaveBuffers* w = b->wave;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int occ_e = 0, occ_s = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e, extend_batch_kernel<false>, WAVE_BLOCK, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, shade_kernel<LAM_QUALITY_MEDIUM, false, false, true>, WAVE_BLOCK, 0);
+    const int grid_e = sms * (int)(t.extend_blocks_per_sm ? std::min<uint32_t>(t.extend_blocks_per_sm, std::max(1, occ_e))
+                                                          : (uint32_t)std::max(1, occ_e));
+    const int grid_s = sms * (int)(t.shade_blocks_per_sm ? t.shade_blocks_per_sm : (uint32_t)std::max(1, occ_s));
+    const BatchPlan P = plan_batch(reqs, n, t.wave_paths);
+    // device tables (uploaded before any capture)
+    if (dgrow(b, &b->reqs, &b->reqs_cap, n) || dgrow(b, &b->segs, &b->segs_cap, P.segs.size()) ||
+        dgrow(b, &b->done, &b->done_cap, n) || dgrow(b, &b->times, &b->times_cap, n + 1) ||
+        dgrow(b, &b->pix_color, &b->pix_cap, P.pixels) || dgrow(b, &b->pixel_seed, &b->seed_cap, P.pixels))
+        return LAM_ERR_CUDA;
+    std::vector<BatchReq> hr(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const lam_batch_request& r = reqs[i];
+        BatchReq& q = hr[i];
+        q.S = r.scene->dev;
+        q.cam = r.camera;
+        q.camera_pos = v3{r.camera.view_inverse[12], r.camera.view_inverse[13], r.camera.view_inverse[14]};
+        q.width = r.targets.width;
+        q.height = r.targets.height;
+        q.npix = q.width * q.height;
+        q.samples = r.samples;
+        q.seed_offset = r.seed_offset;
+        q.pix_base = P.pix_base[i];
+        q.out_color = (float4*)r.targets.color;
+        q.out_normal = (float4*)r.targets.normal;
+        q.out_albedo = (float4*)r.targets.albedo;
+    }
+    cudaError_t e = cudaMemcpy(b->reqs, hr.data(), n * sizeof(BatchReq), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->segs, P.segs.data(), P.segs.size() * sizeof(BatchSeg), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_error(e, "lam_batch_render tables");
+    b->last_n = n;
+    if (!b->stream) {
+        if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming)) != cudaSuccess)
+            return cuda_error(e, "batch stream");
+    }
+    cudaStream_t caller = (cudaStream_t)stream;
+    cudaStream_t st = b->stream;
+    cudaEventRecord(b->ev_in, caller);
+    cudaStreamWaitEvent(st, b->ev_in, 0);
+
+    Args A;
+    std::memset(&A, 0, sizeof(A));
+    A.max_depth = pl->opts.max_depth;
+    A.restir = LAM_RESTIR_DISABLED;
+    A.tmin = pl->opts.tmin;
+    A.tmax = pl->opts.tmax;
+    A.ray_o = w->ray_o;
+    A.ray_d = w->ray_d;
+    A.hit = w->hit;
+    A.err = w->ctr + 4;
+    A.segments = reinterpret_cast<unsigned long long*>(w->ctr + 8);
+    A.thr = w->thr;
+    A.acc = w->acc;
+    A.brdf = w->brdf;
+    A.seed = w->seed;
+    A.flags = w->flags;
+    A.pix_color = b->pix_color;
+    A.pixel_seed = b->pixel_seed;
+    A.reqs = b->reqs;
+    A.req_done = b->done;
+    A.req_time = b->times;
+    const dim3 blk(WAVE_BLOCK);
+    uint32_t launches = 0;
+    auto record = [&]() {
+        cudaMemsetAsync(w->ctr, 0, 10 * sizeof(uint32_t), st);
+        batch_start_kernel<<<1, 256, 0, st>>>(b->done, b->times, n);
+        for (size_t wv = 0; wv < P.wave_begin.size(); ++wv) {
+            A.segs = b->segs + P.wave_begin[wv];
+            A.nsegs = P.wave_nsegs[wv];
+            A.pix_threads = P.wave_threads[wv];
+            A.npix = P.wave_paths[wv];
+            uint32_t* qa = w->queue0;
+            uint32_t* qb = w->queue1;
+            uint32_t* ca = w->ctr + 0;
+            uint32_t* cb = w->ctr + 1;
+            A.q_in = qa;
+            A.count_in = ca;
+            const dim3 gp((A.pix_threads + WAVE_BLOCK - 1) / WAVE_BLOCK);
+            batch_generate_kernel<<<gp, blk, 0, st>>>(A);
+            for (uint32_t depth = 0; depth < pl->opts.max_depth; ++depth) {
+                A.q_in = qa;
+                A.q_out = qb;
+                A.count_in = ca;
+                A.count_out = cb;
+                A.work = w->ctr + 2;
+                cudaMemsetAsync(w->ctr + 2, 0, sizeof(uint32_t), st);
+                cudaMemsetAsync(cb, 0, sizeof(uint32_t), st);
+                if (all_opaque) extend_batch_kernel<false><<<grid_e, blk, 0, st>>>(A);
+                else extend_batch_kernel<true><<<grid_e, blk, 0, st>>>(A);
+                switch (pl->quality) {
+                    case LAM_QUALITY_LOW: shade_kernel<LAM_QUALITY_LOW, false, false, true><<<grid_s, blk, 0, st>>>(A); break;
+                    case LAM_QUALITY_HIGH: shade_kernel<LAM_QUALITY_HIGH, false, false, true><<<grid_s, blk, 0, st>>>(A); break;
+                    default: shade_kernel<LAM_QUALITY_MEDIUM, false, false, true><<<grid_s, blk, 0, st>>>(A); break;
+                }
+                launches += 2;
+                std::swap(qa, qb);
+                std::swap(ca, cb);
+            }
+            batch_accumulate_kernel<<<gp, blk, 0, st>>>(A);
+            launches += 2;
+        }
+    };
+    if (t.use_graph) {
+        std::vector<char> key;
+        batch_key(reqs, n, t, b->generation, key);
+        if (!b->graph || key != b->graph_key) {
+            if (b->graph) cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+            cudaGraph_t g = nullptr;
+            e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return cuda_error(e, "lam_batch_render capture");
+            record();
+            e = cudaStreamEndCapture(st, &g);
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_error(e, "lam_batch_render graph");
+            b->graph_key = key;
+        }
+        e = cudaGraphLaunch(b->graph, st);
+        if (e != cudaSuccess) return cuda_error(e, "lam_batch_render graph launch");
+    } else {
+        record();
+    }
+    cudaEventRecord(b->ev_out, st);
+    cudaStreamWaitEvent(caller, b->ev_out, 0);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_error(e, "lam_batch_render launch");
+    pl->stats.samples = 0;
+    for (uint32_t i = 0; i < n; ++i) pl->stats.samples += (uint64_t)reqs[i].targets.width * reqs[i].targets.height * reqs[i].samples;
+    pl->stats.kernel_launches = launches;
+    pl->stats_ctr = w->ctr;
+    pl->stats_pending = true;
+    return LAM_OK;
+}
+
+extern "C" int lam_batch_latencies(lam_pipeline* pl, uint32_t n, double* ms) {
+    if (!pl || !ms) return set_error(LAM_ERR_INVALID_ARGUMENT, "null argument");
+    BatchState* b = pl->batch;
+    if (!b || b->last_n != n) return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_batch_latencies: n differs from the last batch");
+    std::vector<unsigned long long> h(n + 1);
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(h.data(), b->times, (n + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_error(e, "lam_batch_latencies");
+    for (uint32_t i = 0; i < n; ++i) ms[i] = (double)(long long)(h[i] - h[n]) * 1e-6;
+    return LAM_OK;
+}
+
+extern "C" int lam_batch_autotune(lam_pipeline* pl, const lam_batch_request* reqs, uint32_t n, uint32_t spp_divisor,
+                                  lam_batch_tuning* out, void* stream) {
+    if (!pl || !out || (n && !reqs)) return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_batch_autotune: null argument");
+    std::vector<lam_batch_request> r(reqs, reqs + n);
+    const uint32_t div = std::max(1u, spp_divisor);
+    for (auto& q : r) q.samples = std::max(1u, q.samples / div);
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto timeit = [&](const lam_batch_tuning& t, float* ms) -> int {
+        int rc = lam_batch_render(pl, r.data(), n, &t, stream);  // warm-up (allocations, first touch)
+        if (rc) return rc;
+        cudaEventRecord(e0, st);
+        rc = lam_batch_render(pl, r.data(), n, &t, stream);
+        if (rc) return rc;
+        cudaEventRecord(e1, st);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) return cuda_error(e, "lam_batch_autotune");
+        cudaEventElapsedTime(ms, e0, e1);
+        return LAM_OK;
+    };
+    lam_batch_tuning best{};
+    best.use_graph = 0;
+    float best_ms = 3.0e38f;
+    int rc = LAM_OK;
+    // coordinate 1: queue size
+    for (uint32_t wp : {2u << 20, 4u << 20, 8u << 20, 16u << 20}) {
+        lam_batch_tuning t = best;
+        t.wave_paths = wp;
+        float ms = 0;
+        if ((rc = timeit(t, &ms))) break;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = t;
+        }
+    }
+    // coordinate 2: shade CTAs per SM; coordinate 3: extend CTAs per SM
+    for (int c = 0; c < 2 && rc == LAM_OK; ++c) {
+        lam_batch_tuning base = best;
+        for (uint32_t v : {1u, 2u, 3u, 4u}) {
+            lam_batch_tuning t = base;
+            if (c == 0) t.shade_blocks_per_sm = v;
+            else t.extend_blocks_per_sm = v;
+            float ms = 0;
+            if ((rc = timeit(t, &ms))) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = t;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    best.use_graph = 1;
+    *out = best;
     return LAM_OK;
 }
