@@ -61,6 +61,25 @@ LAM_DEV void setup_ray(TravRay& r, float3 o, float3 d) {
     r.Sz = __fdiv_rn(1.0f, dz);
 }
 
+// setup_ray without the three divisions of the shear constants (restores a ray whose Sx, Sy, Sz
+// are known).
+LAM_DEV void setup_ray_keep_shear(TravRay& r, float3 o, float3 d) {
+    r.o = o;
+    r.d = d;
+    r.inv = make_float3(safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z));
+    r.oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+    float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    int kz = 0;
+    float m = ax;
+    if (ay > m) { kz = 1; m = ay; }
+    if (az > m) kz = 2;
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    float dz = sel3(kz, d.x, d.y, d.z);
+    if (dz < 0.0f) { int t = kx; kx = ky; ky = t; }
+    r.kx = kx; r.ky = ky; r.kz = kz;
+}
+
 LAM_DEV void object_ray(const float* m, float3 o, float3 d, float3* oo, float3* od) {
     oo->x = __fmaf_rn(m[0], o.x, __fmaf_rn(m[1], o.y, __fmaf_rn(m[2], o.z, m[3])));
     oo->y = __fmaf_rn(m[4], o.x, __fmaf_rn(m[5], o.y, __fmaf_rn(m[6], o.z, m[7])));
@@ -227,6 +246,7 @@ template <bool ANY, bool ALPHA>
 struct Traverser {
     TravRay R;
     float3 wo, wd;
+    float wSx, wSy, wSz;  // the world ray's shear constants, restored when an instance is left
     float tmin, best_t;
     uint2 ng, tg;
     int sp, blas_base;
@@ -248,6 +268,9 @@ struct Traverser {
         cur_inst = 0u;
         cur_flags = 0u;
         setup_ray(R, o, d);
+        wSx = R.Sx;
+        wSy = R.Sy;
+        wSz = R.Sz;
         ng = S.tlas_node_count ? make_uint2(0u, (1u << (24u + R.oct)) | 1u) : make_uint2(0u, 0u);
         tg = make_uint2(0u, 0u);
     }
@@ -325,7 +348,10 @@ struct Traverser {
         if (ng.y <= 0x00FFFFFFu) {
             if (blas_base >= 0 && sp == blas_base) {
                 blas_base = -1;
-                setup_ray(R, wo, wd);
+                setup_ray_keep_shear(R, wo, wd);
+                R.Sx = wSx;
+                R.Sy = wSy;
+                R.Sz = wSz;
             }
             if (sp == 0) {
                 res.t = best_t;

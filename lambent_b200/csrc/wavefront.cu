@@ -1508,6 +1508,7 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
     A.out_normal = (float4*)tg->normal;
     A.out_albedo = (float4*)tg->albedo;
     A.camera_pos = v3{cam->view_inverse[12], cam->view_inverse[13], cam->view_inverse[14]};
+    std::memcpy(A.box, s->bounds, sizeof(A.box));
     lam_guide* gd = learned ? pl->guide : nullptr;
     if (gd) {
         A.dq = w->dq;
