@@ -166,6 +166,24 @@ typedef struct lam_blas_desc {
     uint32_t flags;           /* LAM_GEOMETRY_OPAQUE: skip the alpha test (general.wesl:1059-1067) */
 } lam_blas_desc;
 
+/* The no-vertex-return input format (Vertices / Indices, src/lib.rs:439-454, bindings.wesl:83-113,
+ * get_vertices general.wesl): a Vertices blob is geometry_stride (u32) and 12 zero bytes followed by
+ * [f32; 4] vertices; an Indices array of length 1 means "no indices" (the vertex index is used
+ * directly).  Triangle p of geometry g reads the index slots geometry_stride * g + 3p + {0, 1, 2}.
+ * Fills *out with a BLAS whose vertices point into the blob (it must outlive *out) and whose index
+ * list (owned by *out; release it with lam_blas_desc_free) lists the triangles geometry by geometry,
+ * numbered consecutively.  Out-of-range slots or vertex indices: LAM_ERR_INVALID_ARGUMENT. */
+int lam_blas_from_vertices(const void* vertices_blob, size_t blob_bytes, const uint32_t* indices,
+                           size_t index_count, uint32_t geometry_count, const uint32_t* triangles_per_geometry,
+                           uint32_t flags, lam_blas_desc* out);
+int lam_blas_desc_free(lam_blas_desc* desc);
+/* The reference looks materials up by the primitive index within its geometry
+ * (material_idx[instance].materials[primitive_index], general.wesl:1059); writes the table indexed
+ * by the consecutive numbering of lam_blas_from_vertices (out: sum of triangles_per_geometry
+ * entries).  An index past the end of `table` reads its last entry, as a clamped GPU load does. */
+int lam_material_table_for_geometries(const uint32_t* table, uint32_t table_len, uint32_t geometry_count,
+                                      const uint32_t* triangles_per_geometry, uint32_t* out);
+
 /* One top-level instance (TlasInstance::new, main.rs:493-498) plus its material table
  * (binding 0/1 material_idx[instance].materials[primitive], bindings.wesl:59-70). */
 typedef struct lam_instance_desc {

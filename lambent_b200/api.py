@@ -101,6 +101,9 @@ def lib():
     _sig(L, "lam_guide_progress", i, vp, P(C.c_uint64), u32p)
     _sig(L, "lam_pipeline_set_guide", i, vp, vp)
     _sig(L, "lam_scene_bounds", i, vp, f32p)
+    _sig(L, "lam_blas_from_vertices", i, vp, C.c_size_t, u32p, C.c_size_t, u32, u32p, u32, P(_abi.BlasDesc))
+    _sig(L, "lam_blas_desc_free", i, P(_abi.BlasDesc))
+    _sig(L, "lam_material_table_for_geometries", i, u32p, u32, u32, u32p, u32p)
     _sig(L, "lam_batch_render", i, vp, P(_abi.BatchRequest), u32, P(_abi.BatchTuning), vp)
     _sig(L, "lam_batch_latencies", i, vp, u32, P(C.c_double))
     _sig(L, "lam_batch_autotune", i, vp, P(_abi.BatchRequest), u32, u32, P(_abi.BatchTuning), vp)
@@ -629,3 +632,49 @@ class Guide:
         if getattr(self, "_h", None) and _LIB is not None:
             _LIB.lam_guide_destroy(self._h)
             self._h = None
+
+
+# ---------------------------------------------------------------- no-vertex-return input format
+class Vertices:
+    """The reference's Vertices record (src/lib.rs:439-454): geometry_stride and [f32; 4] vertices."""
+
+    def __init__(self, geometry_stride, vertices):
+        import numpy as np
+        self.geometry_stride = int(geometry_stride)
+        self.vertices = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 4)
+
+    def append_bytes(self, out=None):
+        """Vertices::append_bytes: stride (u32), 12 zero bytes, then the vertices."""
+        import numpy as np
+        b = np.uint32(self.geometry_stride).tobytes() + bytes(12) + self.vertices.tobytes()
+        return b if out is None else out + b
+
+
+def blas_from_vertices(vertices_blob, indices, triangles_per_geometry, flags=1):
+    """lam_blas_from_vertices: a BLAS dict (vertices (V, 4), indices, flags) for lambent_b200 scenes."""
+    import numpy as np
+    blob = np.frombuffer(bytes(vertices_blob), dtype=np.uint8).copy()
+    idx = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1)
+    tpg = np.ascontiguousarray(triangles_per_geometry, dtype=np.uint32).reshape(-1)
+    d = _abi.BlasDesc()
+    check(lib().lam_blas_from_vertices(blob.ctypes.data_as(C.c_void_p), blob.size,
+                                       idx.ctypes.data_as(C.POINTER(C.c_uint32)), idx.size, tpg.size,
+                                       tpg.ctypes.data_as(C.POINTER(C.c_uint32)), flags, C.byref(d)))
+    try:
+        v = np.ctypeslib.as_array(d.vertices, shape=(d.vertex_count * 4,)).reshape(-1, 4).copy() if d.vertex_count else \
+            np.zeros((0, 4), np.float32)
+        ix = np.ctypeslib.as_array(d.indices, shape=(d.index_count,)).copy() if d.index_count else np.zeros(0, np.uint32)
+    finally:
+        check(lib().lam_blas_desc_free(C.byref(d)))
+    return {"vertices": v, "indices": ix, "flags": flags}
+
+
+def material_table_for_geometries(table, triangles_per_geometry):
+    import numpy as np
+    t = np.ascontiguousarray(table, dtype=np.uint32).reshape(-1)
+    tpg = np.ascontiguousarray(triangles_per_geometry, dtype=np.uint32).reshape(-1)
+    out = np.zeros(int(tpg.sum()), dtype=np.uint32)
+    check(lib().lam_material_table_for_geometries(t.ctypes.data_as(C.POINTER(C.c_uint32)), t.size, tpg.size,
+                                                  tpg.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                                  out.ctypes.data_as(C.POINTER(C.c_uint32))))
+    return out

@@ -6,6 +6,8 @@
 #include <cstring>
 #include <fstream>
 #include <iterator>
+#include <mutex>
+#include <unordered_set>
 #include <string>
 #include <vector>
 
@@ -366,6 +368,79 @@ int lam_tracer_options_default(lam_tracer_options* o) {
     o->restir_temporal = LAM_RESTIR_PER_PIXEL;
     o->max_depth = 5;
     o->guide_mode = LAM_GUIDE_NONE;
+    return LAM_OK;
+}
+
+// ---------------------------------------------------------------- no-vertex-return input format
+static std::mutex g_desc_mutex;
+static std::unordered_set<const uint32_t*> g_desc_indices;  // index lists owned by adapter descs
+
+int lam_blas_from_vertices(const void* blob, size_t blob_bytes, const uint32_t* indices, size_t index_count,
+                           uint32_t geometry_count, const uint32_t* tris_per_geometry, uint32_t flags,
+                           lam_blas_desc* out) {
+    if (!blob || !out || (geometry_count && !tris_per_geometry))
+        return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_blas_from_vertices: null argument");
+    if (blob_bytes < 16 || (blob_bytes - 16) % 16 != 0)
+        return set_error(LAM_ERR_INVALID_ARGUMENT, "Vertices blob: 16-byte header then [f32; 4] vertices");
+    uint32_t stride;
+    std::memcpy(&stride, blob, 4);
+    const uint64_t vcount = (blob_bytes - 16) / 16;
+    if (vcount > 0xFFFFFFFFull) return set_error(LAM_ERR_INVALID_ARGUMENT, "too many vertices");
+    // arrayLength(&indices) == 1 selects the vertex index itself (get_vertices, general.wesl)
+    const bool direct = !indices || index_count <= 1;
+    uint64_t tris = 0;
+    for (uint32_t g = 0; g < geometry_count; ++g) tris += tris_per_geometry[g];
+    if (tris * 3 > 0xFFFFFFFFull) return set_error(LAM_ERR_INVALID_ARGUMENT, "too many triangles");
+    std::vector<uint32_t> list;
+    list.reserve((size_t)tris * 3);
+    for (uint32_t g = 0; g < geometry_count; ++g)
+        for (uint32_t p = 0; p < tris_per_geometry[g]; ++p)
+            for (uint32_t j = 0; j < 3; ++j) {
+                const uint64_t slot = (uint64_t)stride * g + 3ull * p + j;
+                uint64_t v = slot;
+                if (!direct) {
+                    if (slot >= index_count) return set_error(LAM_ERR_INVALID_ARGUMENT, "index slot past the Indices array");
+                    v = indices[slot];
+                }
+                if (v >= vcount) return set_error(LAM_ERR_INVALID_ARGUMENT, "vertex index past the Vertices blob");
+                list.push_back((uint32_t)v);
+            }
+    uint32_t* owned = new uint32_t[std::max<size_t>(1, list.size())];
+    if (!list.empty()) std::memcpy(owned, list.data(), list.size() * sizeof(uint32_t));
+    {
+        std::lock_guard<std::mutex> lk(g_desc_mutex);
+        g_desc_indices.insert(owned);
+    }
+    out->vertices = reinterpret_cast<const float*>(static_cast<const char*>(blob) + 16);
+    out->vertex_count = (uint32_t)vcount;
+    out->vertex_stride = 4;
+    out->indices = owned;
+    out->index_count = (uint32_t)list.size();
+    out->flags = flags;
+    return LAM_OK;
+}
+
+int lam_blas_desc_free(lam_blas_desc* d) {
+    if (!d || !d->indices) return LAM_OK;
+    std::lock_guard<std::mutex> lk(g_desc_mutex);
+    auto it = g_desc_indices.find(d->indices);
+    if (it == g_desc_indices.end())
+        return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_blas_desc_free: not made by lam_blas_from_vertices");
+    g_desc_indices.erase(it);
+    delete[] d->indices;
+    d->indices = nullptr;
+    d->index_count = 0;
+    return LAM_OK;
+}
+
+int lam_material_table_for_geometries(const uint32_t* table, uint32_t table_len, uint32_t geometry_count,
+                                      const uint32_t* tris_per_geometry, uint32_t* out) {
+    if (!out || (geometry_count && !tris_per_geometry) || (table_len && !table))
+        return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_material_table_for_geometries: null argument");
+    if (table_len == 0) return set_error(LAM_ERR_INVALID_ARGUMENT, "empty material table");
+    size_t k = 0;
+    for (uint32_t g = 0; g < geometry_count; ++g)
+        for (uint32_t p = 0; p < tris_per_geometry[g]; ++p) out[k++] = table[p < table_len ? p : table_len - 1];
     return LAM_OK;
 }
 
