@@ -16,6 +16,7 @@
 
 #include <stddef.h>
 #include <stdint.h>
+#include "lambent_handler.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -164,6 +165,11 @@ typedef struct lam_blas_desc {
     const uint32_t* indices;  /* NULL: non-indexed, triangle i = vertices 3i..3i+2 */
     uint32_t index_count;     /* multiple of 3 (or 3 * triangle count when non-indexed) */
     uint32_t flags;           /* LAM_GEOMETRY_OPAQUE: skip the alpha test (general.wesl:1059-1067) */
+    /* Procedural geometry instead of triangles (AABB geometry of a BLAS): aabb_count boxes of
+     * 6 floats (min xyz, max xyz).  Candidates go to the pipeline's intersection handler; without
+     * one they miss, as the reference's default handler does. */
+    const float* aabbs;
+    uint32_t aabb_count;
 } lam_blas_desc;
 
 /* The no-vertex-return input format (Vertices / Indices, src/lib.rs:439-454, bindings.wesl:83-113,
@@ -372,10 +378,14 @@ int lam_pipeline_layout_destroy(lam_pipeline_layout* layout);
 /* RayTracer::<S>::new, src/lib.rs:268-279 (quality = LAM_QUALITY_* or LAM_DEBUG_*) */
 int lam_tracer_create(uint32_t quality, lam_tracer** out);
 /* RayTracer::set_intersection_handler, src/lib.rs:291-295 / IntersectionHandler,
- * src/low_level.rs:115-147.  cuda_source defines
- *   __device__ lam_aabb_intersection intersect(const lam_ray_intersection&);
- * It is called for procedural candidates.  NULL restores the default handler
- * (always a miss, src/default_intersection_handler.wesl). */
+ * src/low_level.rs:115-147.  cuda_source (CUDA C++) defines
+ *   __device__ lam_aabb_intersection intersect(const lam_ray_intersection& i);
+ * with the types of lambent_handler.h (included for it).  It is called for every candidate of
+ * procedural (AABB) geometry and must return in finite time.  Pipelines created from the tracer
+ * afterwards compile it with NVRTC and link it into their traversal kernels (nvJitLink);
+ * a source that does not compile fails lam_tracer_create_pipeline with LAM_ERR_COMPILE and the
+ * compiler's log.  NULL restores the default handler (always a miss,
+ * src/default_intersection_handler.wesl). */
 int lam_tracer_set_intersection_handler(lam_tracer* tracer, const char* cuda_source);
 int lam_tracer_destroy(lam_tracer* tracer);
 /* RayTracingOptions::default / PathTracerOpts::default (low_level.rs:101-113) */
@@ -398,6 +408,14 @@ int lam_scene_destroy(lam_scene* scene);
  * general.wesl:1053-1078) for n rays held in device memory. */
 int lam_trace_rays(const lam_scene* scene, const lam_ray* rays, uint32_t n, uint32_t mode,
                    lam_hit* hits, void* stream);
+
+/* lam_trace_rays with the pipeline's intersection handler for procedural geometry (the reference
+ * runs its ray queries inside the pipeline that holds the handler).  Procedural hits report the
+ * handler's t, u = v = 0 and LAM_HIT_BACK (the reference's generated intersections carry no
+ * barycentrics or facing).  Without a handler, or for scenes without procedural geometry, this is
+ * lam_trace_rays. */
+int lam_pipeline_trace_rays(lam_pipeline* pipeline, const lam_scene* scene, const lam_ray* rays, uint32_t n,
+                            uint32_t mode, lam_hit* hits, void* stream);
 
 /* Allocation-free form of lam_trace_rays; it has no counterpart in the reference.  For callers
  * that cannot allocate device memory while they run (a render loop inside a fixed frame budget,

@@ -20,7 +20,9 @@ ERR_INVALID_ARGUMENT = -1
 ERR_PROJECTION_UNINVERTIBLE = -5
 ERR_VIEW_UNINVERTIBLE = -6
 ERR_TEXTURE = -7
+ERR_COMPILE = -8
 ERR_LAYOUT_MISMATCH = -9
+ERR_UNSUPPORTED = -10
 
 DIFFUSE, METALLIC, TRANSPARENT, SKY = 0, 1, 2, 0xFF
 QUALITY_LOW, QUALITY_MEDIUM, QUALITY_HIGH = 0, 1, 2
@@ -72,7 +74,8 @@ class BufferDescriptor(C.Structure):
 
 class BlasDesc(C.Structure):
     _fields_ = [("vertices", C.POINTER(f32)), ("vertex_count", u32), ("vertex_stride", u32),
-                ("indices", C.POINTER(u32)), ("index_count", u32), ("flags", u32)]
+                ("indices", C.POINTER(u32)), ("index_count", u32), ("flags", u32),
+                ("aabbs", C.POINTER(f32)), ("aabb_count", u32)]
 
 
 class InstanceDesc(C.Structure):
@@ -170,6 +173,18 @@ class SceneDescHolder:
         self._keep = []
         blas = (BlasDesc * max(1, len(scene.blas)))()
         for i, b in enumerate(scene.blas):
+            if b.get("aabbs") is not None:  # procedural geometry: (N, 6) boxes, min xyz / max xyz
+                a = np.ascontiguousarray(b["aabbs"], dtype=np.float32).reshape(-1, 6)
+                self._keep.append(a)
+                blas[i].vertices = None
+                blas[i].vertex_count = 0
+                blas[i].vertex_stride = 3
+                blas[i].indices = None
+                blas[i].index_count = 0
+                blas[i].aabbs = a.ctypes.data_as(C.POINTER(f32))
+                blas[i].aabb_count = a.shape[0]
+                blas[i].flags = b.get("flags", GEOMETRY_OPAQUE)
+                continue
             v = np.ascontiguousarray(b["vertices"], dtype=np.float32)
             idx = b.get("indices")
             self._keep.append(v)

@@ -101,6 +101,7 @@ def lib():
     _sig(L, "lam_guide_progress", i, vp, P(C.c_uint64), u32p)
     _sig(L, "lam_pipeline_set_guide", i, vp, vp)
     _sig(L, "lam_scene_bounds", i, vp, f32p)
+    _sig(L, "lam_pipeline_trace_rays", i, vp, vp, vp, u32, u32, vp, vp)
     _sig(L, "lam_blas_from_vertices", i, vp, C.c_size_t, u32p, C.c_size_t, u32, u32p, u32, P(_abi.BlasDesc))
     _sig(L, "lam_blas_desc_free", i, P(_abi.BlasDesc))
     _sig(L, "lam_material_table_for_geometries", i, u32p, u32, u32, u32p, u32p)
@@ -423,6 +424,11 @@ class Pipeline:
 
     def profile_reset(self):
         check(lib().lam_render_profile_reset(self._h))
+
+    def trace_rays(self, scene, rays, hits, mode=_abi.TRACE_CLOSEST, stream=None):
+        """lam_pipeline_trace_rays: ray queries that run the pipeline's intersection handler."""
+        check(lib().lam_pipeline_trace_rays(self._h, scene._h, C.c_void_p(rays.data_ptr()), rays.shape[0], mode,
+                                            C.c_void_p(hits.data_ptr()), _stream_ptr(stream)))
 
     def batch_render(self, requests, tuning=None, stream=None):
         """requests: list of (GpuScene, Camera, FrameTargets, samples, seed_offset).  Renders all of them as

@@ -78,8 +78,20 @@ extern "C" int lam_scene_create(const lam_scene_desc* d, void* stream, lam_scene
     // ---- validate and gather triangles per BLAS
     const uint32_t nb = d->blas_count;
     std::vector<uint32_t> tri_count(nb);
+    std::vector<char> procedural(nb, 0);
     for (uint32_t b = 0; b < nb; ++b) {
         const lam_blas_desc& bd = d->blas[b];
+        if (bd.aabb_count) {
+            if (!bd.aabbs) return set_error(LAM_ERR_INVALID_ARGUMENT, "null aabbs");
+            if (bd.index_count) return set_error(LAM_ERR_INVALID_ARGUMENT, "a BLAS holds triangles or AABBs, not both");
+            for (uint32_t i = 0; i < bd.aabb_count; ++i)
+                for (int k = 0; k < 3; ++k)
+                    if (!(bd.aabbs[6 * (size_t)i + k] <= bd.aabbs[6 * (size_t)i + 3 + k]))
+                        return set_error(LAM_ERR_INVALID_ARGUMENT, "AABB with min > max or NaN");
+            procedural[b] = 1;
+            tri_count[b] = bd.aabb_count;
+            continue;
+        }
         if (bd.vertex_stride != 3 && bd.vertex_stride != 4)
             return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_blas_desc.vertex_stride must be 3 or 4");
         if (bd.index_count % 3 != 0) return set_error(LAM_ERR_INVALID_ARGUMENT, "index_count must be a multiple of 3");
@@ -113,6 +125,23 @@ extern "C" int lam_scene_create(const lam_scene_desc* d, void* stream, lam_scene
                     return bd.vertices + (size_t)vi * bd.vertex_stride;
                 };
                 std::vector<float> boxes(6 * (size_t)n);
+                if (procedural[b]) {
+                    // AABB primitives: leaf slots hold (min, prim bits), (max, 0), (0)
+                    std::memcpy(boxes.data(), bd.aabbs, boxes.size() * sizeof(float));
+                    build_bvh8(boxes.data(), n, 3, &bvh[b]);
+                    std::vector<float4>& td = tri_data[b];
+                    td.resize(3 * (size_t)bvh[b].leaf_items.size());
+                    for (size_t j = 0; j < bvh[b].leaf_items.size(); ++j) {
+                        uint32_t t = bvh[b].leaf_items[j];
+                        const float* a = bd.aabbs + 6 * (size_t)t;
+                        float primbits;
+                        std::memcpy(&primbits, &t, 4);
+                        td[3 * j + 0] = make_float4(a[0], a[1], a[2], primbits);
+                        td[3 * j + 1] = make_float4(a[3], a[4], a[5], 0.0f);
+                        td[3 * j + 2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    }
+                    continue;
+                }
                 for (uint32_t t = 0; t < n; ++t) {
                     for (int k = 0; k < 3; ++k) {
                         float lo = vtx(t, 0)[k], hi = lo;
@@ -169,7 +198,9 @@ extern "C" int lam_scene_create(const lam_scene_desc* d, void* stream, lam_scene
     std::vector<DevInstance> inst(ni);
     std::vector<uint32_t> mat_idx;
     std::vector<float> iboxes(6 * (size_t)ni);
-    bool all_opaque = true;
+    // per instance: object-to-world 3x4, custom index bits, 3 zeros (read by intersection handlers)
+    std::vector<float> fwd(16 * (size_t)ni);
+    bool all_opaque = true, any_procedural = false;
     for (uint32_t i = 0; i < ni; ++i) {
         const lam_instance_desc& id = d->instances[i];
         if (id.blas >= nb) return set_error(LAM_ERR_INVALID_ARGUMENT, "instance references a missing BLAS");
@@ -181,16 +212,28 @@ extern "C" int lam_scene_create(const lam_scene_desc* d, void* stream, lam_scene
         if (I.mat_count) mat_idx.insert(mat_idx.end(), id.material_indices, id.material_indices + I.mat_count);
         bool opaque = (d->blas[id.blas].flags & LAM_GEOMETRY_OPAQUE) != 0u;
         all_opaque = all_opaque && opaque;
-        I.flags = (opaque ? INST_OPAQUE : 0u) | ((id.mask & 0xFFu) ? INST_VISIBLE : 0u);
+        I.flags = (opaque ? INST_OPAQUE : 0u) | ((id.mask & 0xFFu) ? INST_VISIBLE : 0u) |
+                  (procedural[id.blas] ? INST_PROCEDURAL : 0u);
+        any_procedural = any_procedural || procedural[id.blas];
+        std::copy(id.transform, id.transform + 12, fwd.begin() + 16 * (size_t)i);
+        std::memcpy(&fwd[16 * (size_t)i + 12], &id.custom_index, 4);
         // exact world box of the instance's transformed vertices (FP64), padded outward; a box of the
         // rotated object-space bounds would be up to 3^1.5 times larger and admit many rays that
         // cannot hit the instance
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
         const lam_blas_desc& bd = d->blas[id.blas];
-        const uint32_t nidx = tri_count[id.blas] * 3u;
+        const uint32_t nidx = procedural[id.blas] ? bd.aabb_count * 8u : tri_count[id.blas] * 3u;
         for (uint32_t k = 0; k < nidx; ++k) {
-            const uint32_t vi = bd.indices ? bd.indices[k] : k;
-            const float* pv = bd.vertices + (size_t)vi * bd.vertex_stride;
+            float corner[3];
+            const float* pv;
+            if (procedural[id.blas]) {  // the 8 corners of every box
+                const float* a = bd.aabbs + 6 * (size_t)(k >> 3);
+                for (int c = 0; c < 3; ++c) corner[c] = a[((k >> c) & 1u) ? 3 + c : c];
+                pv = corner;
+            } else {
+                const uint32_t vi = bd.indices ? bd.indices[k] : k;
+                pv = bd.vertices + (size_t)vi * bd.vertex_stride;
+            }
             for (int r = 0; r < 3; ++r) {
                 const float* q = id.transform + 4 * r;
                 double w = (double)q[0] * pv[0] + (double)q[1] * pv[1] + (double)q[2] * pv[2] + (double)q[3];
@@ -259,6 +302,7 @@ extern "C" int lam_scene_create(const lam_scene_desc* d, void* stream, lam_scene
     if ((rc = upload(s, d->materials, d->material_count, &D.materials, st))) return fail(rc);
     if ((rc = upload(s, texels.data(), texels.size(), &D.texels, st))) return fail(rc);
     if ((rc = upload(s, layers.data(), layers.size(), &D.layers, st))) return fail(rc);
+    if (any_procedural && (rc = upload(s, fwd.data(), fwd.size(), &D.inst_fwd, st))) return fail(rc);
     if (d->sky_faces && d->sky_size) {
         size_t n = 6 * (size_t)d->sky_size * d->sky_size;
         std::vector<uint32_t> sky(n);
@@ -277,6 +321,7 @@ extern "C" int lam_scene_create(const lam_scene_desc* d, void* stream, lam_scene
     D.tlas_node_count = (uint32_t)tlas.nodes.size();
     D.instance_count = ni;
     D.all_opaque = all_opaque ? 1u : 0u;
+    D.has_procedural = any_procedural ? 1u : 0u;
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail(cuda_error(e, "scene upload"));
     s->blas_count = nb;

@@ -19,7 +19,7 @@ struct DevInstance {
     uint32_t flags;       // INST_OPAQUE | INST_VISIBLE
 };
 static_assert(sizeof(DevInstance) == 64, "instance record is 64 bytes");
-enum : uint32_t { INST_OPAQUE = 1u, INST_VISIBLE = 2u };
+enum : uint32_t { INST_OPAQUE = 1u, INST_VISIBLE = 2u, INST_PROCEDURAL = 4u };
 
 struct DevTexLayer {
     uint32_t offset;      // first texel (RGBA8 as u32) in the texel pool
@@ -47,6 +47,8 @@ struct DevScene {
     uint32_t tlas_node_count;
     uint32_t instance_count;
     uint32_t all_opaque;
+    uint32_t has_procedural;      // some instance holds AABB geometry
+    const float* inst_fwd;        // per instance: object-to-world 3x4, custom index, 3 zeros (procedural scenes)
 };
 
 }  // namespace lam

@@ -36,6 +36,14 @@ struct lam_data_buffers {
 namespace lam {
 
 struct WaveBuffers;  // defined in wavefront.cu
+// A pipeline's intersection handler, linked into the procedural traversal kernels (handler_jit.cpp).
+struct HandlerModule {
+    cudaLibrary_t lib = nullptr;
+    cudaKernel_t extend = nullptr, trace_closest = nullptr, trace_any = nullptr;
+};
+int compile_handler_cubin(const std::string& source, std::vector<char>* cubin, std::string* log);
+int load_handler_module(const std::vector<char>& cubin, HandlerModule* m);
+void free_handler_module(HandlerModule* m);
 struct BatchState;   // defined in wavefront.cu
 void free_batch(BatchState* b);
 
@@ -62,6 +70,8 @@ struct lam_pipeline {
     uint64_t prof_segments_base = 0;
     uint64_t total_segments = 0;
     lam_guide* guide = nullptr;  // learned guide (not owned)
+    std::vector<char> handler_cubin;   // intersection handler linked with the procedural kernels
+    lam::HandlerModule* handler = nullptr;  // loaded on first use
     lam::BatchState* batch = nullptr;  // lam_batch_render state
     uint32_t* stats_ctr = nullptr;     // device counters of the last render (single or batched)
 };

@@ -233,7 +233,28 @@ struct TraceResult {
     uint32_t inst;
     uint32_t prim;
     float t;        // f32 watertight distance
+#ifdef LAM_HAVE_HANDLER
+    float3 pn, ptg; // normal and tangent of a committed procedural hit (from the handler)
+#endif
 };
+
+}  // namespace lam
+#ifdef LAM_HAVE_HANDLER
+// The intersection handler, linked in at run time (lam_tracer_set_intersection_handler).
+extern "C" __device__ lam_aabb_intersection lam_user_intersect(const lam_ray_intersection& i);
+#endif
+namespace lam {
+
+// Conservative ray / box test in the ray's own space (procedural candidates reach the handler only
+// when the ray crosses their box inside (tmin, limit), as the driver's AABB candidates do).
+LAM_DEV bool ray_box(const TravRay& r, float4 lo, float4 hi, float tmin, float limit) {
+    const float tx0 = (lo.x - r.o.x) * r.inv.x, tx1 = (hi.x - r.o.x) * r.inv.x;
+    const float ty0 = (lo.y - r.o.y) * r.inv.y, ty1 = (hi.y - r.o.y) * r.inv.y;
+    const float tz0 = (lo.z - r.o.z) * r.inv.z, tz1 = (hi.z - r.o.z) * r.inv.z;
+    const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+    const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), limit));
+    return tn <= tf * 1.00000095367431640625f;
+}
 
 // Alpha-test callback for non-opaque geometry: candidate accepted unless the diffuse texel's
 // alpha is near zero, transparent materials always accepted (general.wesl:1059-1067).
@@ -323,6 +344,54 @@ struct Traverser {
                 return true;
             }
             const float4* tp = S.tris + 3u * item;
+            if (cur_flags & INST_PROCEDURAL) {
+#ifdef LAM_HAVE_HANDLER
+                const float4 lo = __ldg(tp), hi = __ldg(tp + 1);
+                if (!ray_box(R, lo, hi, tmin, best_t)) continue;
+                const uint32_t prim = __float_as_uint(lo.w);
+                lam_ray_intersection ri;
+                ri.kind = LAM_INTERSECTION_AABB;
+                ri.t = best_t;
+                const float* fw = S.inst_fwd + 16u * cur_inst;
+                ri.instance_custom_data = __float_as_uint(fw[12]);
+                ri.instance_index = cur_inst;
+                ri.sbt_record_offset = 0u;
+                ri.geometry_index = 0u;
+                ri.primitive_index = prim;
+                ri.barycentrics[0] = 0.0f;
+                ri.barycentrics[1] = 0.0f;
+                ri.front_face = 0u;
+#pragma unroll
+                for (int q = 0; q < 12; ++q) {
+                    ri.object_to_world[q] = fw[q];
+                    ri.world_to_object[q] = insts[cur_inst].inv[q];
+                }
+                ri.world_origin[0] = wo.x; ri.world_origin[1] = wo.y; ri.world_origin[2] = wo.z;
+                ri.world_direction[0] = wd.x; ri.world_direction[1] = wd.y; ri.world_direction[2] = wd.z;
+                ri.object_origin[0] = R.o.x; ri.object_origin[1] = R.o.y; ri.object_origin[2] = R.o.z;
+                ri.object_direction[0] = R.d.x; ri.object_direction[1] = R.d.y; ri.object_direction[2] = R.d.z;
+                ri.tmin = tmin;
+                ri.aabb_min[0] = lo.x; ri.aabb_min[1] = lo.y; ri.aabb_min[2] = lo.z;
+                ri.aabb_max[0] = hi.x; ri.aabb_max[1] = hi.y; ri.aabb_max[2] = hi.z;
+                const lam_aabb_intersection ai = lam_user_intersect(ri);
+                const float t = ai.t;
+                const bool better = ai.hit && t > tmin &&
+                                    (t < best_t || (t == best_t && res.tri != NO_HIT &&
+                                                    (cur_inst < res.inst || (cur_inst == res.inst && prim < res.prim))));
+                if (!better) continue;
+                best_t = t;
+                res.tri = item;
+                res.inst = cur_inst;
+                res.prim = prim;
+                res.pn = make_float3(ai.normal[0], ai.normal[1], ai.normal[2]);
+                res.ptg = make_float3(ai.tangent[0], ai.tangent[1], ai.tangent[2]);
+                if (ANY) {
+                    res.t = best_t;
+                    return false;
+                }
+#endif
+                continue;
+            }
             const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
             float t;
             if (!wbw_f32(R, a, b, c, best_t, &t)) continue;

@@ -19,11 +19,10 @@
 #include "scene.h"
 #include "tracer.h"
 #include "traverse.cuh"
+#include "wavefront.cuh"
 
 namespace lam {
 
-constexpr int WAVE_BLOCK = 128;
-constexpr uint32_t NO_REC = 0xFFFFFFFFu;
 
 struct Isect {
     v3 color;
@@ -38,17 +37,40 @@ struct Isect {
 };
 
 // ray_hit's post-query part (general.wesl:1080-1137) for a committed triangle.
-LAM_DEV void make_isect(const DevScene& S, const DevInstance* insts, uint2 hit, float3 o, float3 d, Isect& r) {
-    float m[12];
-#pragma unroll
-    for (int q = 0; q < 12; ++q) m[q] = insts[hit.y].inv[q];
-    float3 oo, od;
-    object_ray(m, o, d, &oo, &od);
+// A committed procedural hit is a generated intersection (general.wesl:1068-1075, 1100-1102): the
+// handler's t, normal and tangent (phit_a = normal, t; phit_b = tangent), barycentrics 0, back face.
+LAM_DEV void make_isect(const DevScene& S, const DevInstance* insts, uint2 hit, float3 o, float3 d, Isect& r,
+                        const float4* phit_a = nullptr, const float4* phit_b = nullptr, uint32_t path = 0u) {
     const float4* tp = S.tris + 3u * hit.x;
-    const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+    const float4 a = __ldg(tp);
     float t, bu, bv;
     bool front;
-    wbw_f64(oo, od, a, b, c, &t, &bu, &bv, &front);
+    v3 tg, n;
+    if (phit_a && (insts[hit.y].flags & INST_PROCEDURAL)) {
+        const float4 pa = phit_a[path], pb = phit_b[path];
+        t = pa.w;
+        bu = bv = 0.0f;
+        front = false;
+        n = mk(pa.x, pa.y, pa.z);
+        tg = mk(pb.x, pb.y, pb.z);
+    } else {
+        float m[12];
+#pragma unroll
+        for (int q = 0; q < 12; ++q) m[q] = insts[hit.y].inv[q];
+        float3 oo, od;
+        object_ray(m, o, d, &oo, &od);
+        const float4 b = __ldg(tp + 1), c = __ldg(tp + 2);
+        wbw_f64(oo, od, a, b, c, &t, &bu, &bv, &front);
+        v3 v0 = mk(a.x, a.y, a.z), v1 = mk(b.x, b.y, b.z), v2 = mk(c.x, c.y, c.z);
+        tg = normalize(v0 - v1);
+        {
+            float ax = fabsf(tg.x), ay = fabsf(tg.y), az = fabsf(tg.z);
+            bool xl = ax > ay && ax > az, yl = ay > ax && ay > az;
+            bool rev = xl ? tg.x < 0.0f : (yl ? tg.y < 0.0f : tg.z < 0.0f);
+            if (rev) tg = -tg;
+        }
+        n = normalize(cross(tg, v0 - v2));
+    }
     r.t = t;
     r.front_face = front;
     const uint32_t prim = __float_as_uint(a.w);
@@ -59,15 +81,6 @@ LAM_DEV void make_isect(const DevScene& S, const DevInstance* insts, uint2 hit, 
     float2 ri = unpack2x16float(mt.refractive_index);
     r.ior_low = ri.x;
     r.ior_high = ri.y;
-    v3 v0 = mk(a.x, a.y, a.z), v1 = mk(b.x, b.y, b.z), v2 = mk(c.x, c.y, c.z);
-    v3 tg = normalize(v0 - v1);
-    {
-        float ax = fabsf(tg.x), ay = fabsf(tg.y), az = fabsf(tg.z);
-        bool xl = ax > ay && ax > az, yl = ay > ax && ay > az;
-        bool rev = xl ? tg.x < 0.0f : (yl ? tg.y < 0.0f : tg.z < 0.0f);
-        if (rev) tg = -tg;
-    }
-    v3 n = normalize(cross(tg, v0 - v2));
     v3 dw = mk(d.x, d.y, d.z);
     r.normal = dot(dw, n) > 0.0f ? -n : n;
     r.tangent = tg;
@@ -172,6 +185,7 @@ struct WaveBuffers {
     uint32_t* dq = nullptr;
     float4 *def_n = nullptr, *def_t = nullptr, *def_c = nullptr;
     uint32_t* rec_head = nullptr;
+    float4 *phit_a = nullptr, *phit_b = nullptr;  // procedural hits (allocated on first use)
     uint32_t* ctr = nullptr;  // [0..1] queue counts, [2..3] work counters, [4] error flags,
                               // [8..11] segment counters, [12] diffuse-queue count, [13] records
     std::vector<void*> allocs;
@@ -193,74 +207,6 @@ static int walloc(WaveBuffers* w, T** p, size_t count) {
     w->allocs.push_back(*p);
     return LAM_OK;
 }
-
-// ---------------------------------------------------------------- batched renders
-// A request of lam_batch_render: its scene, camera, image and samples.
-struct BatchReq {
-    DevScene S;
-    lam_camera cam;
-    v3 camera_pos;
-    uint32_t width, height, npix, samples, seed_offset;
-    uint32_t pix_base;  // first entry of this request's pixels in the batch's per-pixel pools
-    float4 *out_color, *out_normal, *out_albedo;
-};
-// A segment of a wave: `count` consecutive samples (from `first`) of every pixel of one request,
-// as paths path_base + s * npix + pixel.
-struct BatchSeg {
-    uint32_t req, first, count, path_base;
-    uint32_t pix_thread_base;  // first generate/accumulate thread of the segment within its wave
-};
-
-// ---------------------------------------------------------------- kernel arguments
-struct Args {
-    DevScene S;
-    lam_camera cam;
-    uint32_t width, height, npix, samples, max_depth, restir, seed_offset;
-    float tmin, tmax;
-    uint32_t wave_first, wave_count;
-    // wave buffers
-    float4 *ray_o, *ray_d;
-    uint2* hit;
-    uint32_t *q_in, *q_out;
-    uint32_t *count_in, *count_out, *work;
-    uint32_t* err;
-    unsigned long long* segments;
-    float4 *thr, *acc;
-    float* brdf;
-    uint32_t *seed, *flags;
-    float4 *ort, *orad, *ppoint, *pnormal, *vpoint, *vnormal, *lnormal, *ldir;
-    float4 *pix_color, *pix_orad, *pix_emission, *pix_albedo;
-    lam_markov_chain *tent_snap, *tent_live;
-    // data buffers
-    const lam_markov_chain* old_chains;
-    lam_markov_chain* chains;
-    uint64_t chains_len, old_chains_len;
-    uint32_t* world;
-    const uint32_t* old_world;
-    uint64_t world_len;
-    lam_reservoir* reservoirs;
-    lam_info* info;
-    uint32_t* pixel_seed;
-    // outputs
-    float4 *out_color, *out_normal, *out_albedo;
-    v3 camera_pos;
-    // learned guiding
-    uint32_t *dq, *dq_count;
-    float4 *def_n, *def_t, *def_c;
-    float* recs;             // training records (GUIDE_RECORD_STRIDE floats), null when not training
-    uint32_t rec_cap;
-    float rec_prob;          // probability that a deferred vertex is recorded
-    uint32_t *rec_count, *rec_head;
-    const uint16_t* guide_w; // packed BF16 weights
-    float guide_frac;
-    float box[6];
-    // batched renders
-    const BatchReq* reqs;
-    const BatchSeg* segs;    // this wave's segments
-    uint32_t nsegs, pix_threads;
-    uint32_t* req_done;      // per request: pixels finished
-    unsigned long long* req_time;  // per request: global timer at completion; [n] = batch start
-};
 
 LAM_DEV void create_ray(const Args& A, uint32_t x, uint32_t y, v3* o, v3* d) {
     float hx = __uint2float_rn(A.width) / 2.0f, hy = __uint2float_rn(A.height) / 2.0f;
@@ -517,7 +463,8 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(const __grid_constant
             bool terminated = false;
             if (h.x != NO_HIT) {
                 Isect is;
-                make_isect(S, S.inst, h, make_float3(ro.x, ro.y, ro.z), make_float3(rd.x, rd.y, rd.z), is);
+                make_isect(S, S.inst, h, make_float3(ro.x, ro.y, ro.z), make_float3(rd.x, rd.y, rd.z), is, A.phit_a,
+                           A.phit_b, path);
                 v3 new_pos = fma3(rd, splat(is.t), ro);
                 if (depth != 0u) {
                     v3 est = GUIDE ? grid_radiance(G, new_pos, is.normal, rd) : splat(0.0f);
@@ -1185,6 +1132,18 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
     return LAM_OK;
 }
 
+int ensure_handler(lam_pipeline* pl) {
+    if (pl->handler) return LAM_OK;
+    HandlerModule* m = new HandlerModule();
+    int rc = load_handler_module(pl->handler_cubin, m);
+    if (rc) {
+        free_handler_module(m);
+        return rc;
+    }
+    pl->handler = m;
+    return LAM_OK;
+}
+
 template <int Q>
 static void launch_guide(bool net, int grid, cudaStream_t st, const Args& A) {
     if (net) guide_sample_kernel<Q, true><<<grid, WAVE_BLOCK, GUIDE_SMEM, st>>>(A);
@@ -1343,6 +1302,14 @@ extern "C" int lam_tracer_create_pipeline(const lam_tracer* t, const lam_pipelin
     p->layout = *layout;
     p->intersection_handler = t->intersection_handler;
     cudaGetDevice(&p->device);
+    if (!p->intersection_handler.empty()) {
+        std::string log;
+        int rc = compile_handler_cubin(p->intersection_handler, &p->handler_cubin, &log);
+        if (rc) {
+            delete p;
+            return set_error(rc, log);
+        }
+    }
     *out = p;
     return LAM_OK;
 }
@@ -1351,6 +1318,7 @@ extern "C" int lam_pipeline_destroy(lam_pipeline* p) {
     if (!p) return LAM_OK;
     free_wave(p->wave);
     free_batch(p->batch);
+    free_handler_module(p->handler);
     for (auto& t : p->timed) {
         cudaEventDestroy(t.start);
         cudaEventDestroy(t.end);
@@ -1509,6 +1477,15 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
     A.out_albedo = (float4*)tg->albedo;
     A.camera_pos = v3{cam->view_inverse[12], cam->view_inverse[13], cam->view_inverse[14]};
     std::memcpy(A.box, s->bounds, sizeof(A.box));
+    // procedural geometry with a handler: the run-time-linked extend kernel
+    const bool proc = s->dev.has_procedural && !pl->handler_cubin.empty();
+    if (proc) {
+        if ((rc = ensure_handler(pl))) return rc;
+        if (!w->phit_a && (walloc(w, &w->phit_a, w->paths) || walloc(w, &w->phit_b, w->paths)))
+            return LAM_ERR_CUDA;
+        A.phit_a = w->phit_a;
+        A.phit_b = w->phit_b;
+    }
     lam_guide* gd = learned ? pl->guide : nullptr;
     if (gd) {
         A.dq = w->dq;
@@ -1583,8 +1560,14 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
             cudaMemsetAsync(w->ctr + 2, 0, sizeof(uint32_t), st);
             cudaMemsetAsync(cb, 0, sizeof(uint32_t), st);
             h = begin(1);
-            if (alpha) extend_kernel<true><<<w->grid_extend, blk, 0, st>>>(A);
-            else extend_kernel<false><<<w->grid_extend, blk, 0, st>>>(A);
+            if (proc) {
+                void* kargs[] = {&A};
+                cudaLaunchKernel((const void*)pl->handler->extend, dim3(w->grid_extend), blk, kargs, 0, st);
+            } else if (alpha) {
+                extend_kernel<true><<<w->grid_extend, blk, 0, st>>>(A);
+            } else {
+                extend_kernel<false><<<w->grid_extend, blk, 0, st>>>(A);
+            }
             end(h);
             h = begin(2);
             if (gd) cudaMemsetAsync(w->ctr + 12, 0, sizeof(uint32_t), st);
@@ -1806,6 +1789,8 @@ extern "C" int lam_batch_render(lam_pipeline* pl, const lam_batch_request* reqs,
         if (sc->instance_count > pl->layout.blas_count || sc->diffuse_count > pl->layout.diffuse_count ||
             sc->emission_count > pl->layout.emission_count || sc->attribute_count > pl->layout.attribute_count)
             return set_error(LAM_ERR_LAYOUT_MISMATCH, "a request's scene exceeds the pipeline layout counts");
+        if (sc->dev.has_procedural && !pl->handler_cubin.empty())
+            return set_error(LAM_ERR_UNSUPPORTED, "batched renders do not run intersection handlers");
         max_pix = std::max(max_pix, r.targets.width * r.targets.height);
         all_opaque = all_opaque && sc->dev.all_opaque;
     }
@@ -2031,5 +2016,40 @@ extern "C" int lam_batch_autotune(lam_pipeline* pl, const lam_batch_request* req
     if (rc) return rc;
     best.use_graph = 1;
     *out = best;
+    return LAM_OK;
+}
+
+extern "C" int lam_pipeline_trace_rays(lam_pipeline* pl, const lam_scene* s, const lam_ray* rays, uint32_t n,
+                                       uint32_t mode, lam_hit* hits, void* stream) {
+    if (!pl || !s || (n && (!rays || !hits))) return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_pipeline_trace_rays: null argument");
+    if (!s->dev.has_procedural || pl->handler_cubin.empty()) return lam_trace_rays(s, rays, n, mode, hits, stream);
+    if (mode != LAM_TRACE_CLOSEST && mode != LAM_TRACE_ANY)
+        return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_pipeline_trace_rays: unknown mode");
+    if (n == 0) return LAM_OK;
+    int rc = ensure_handler(pl);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    uint32_t* scratch = nullptr;  // [0] work counter, [1] error flags
+    cudaError_t e = cudaMallocAsync((void**)&scratch, 8, st);
+    if (e != cudaSuccess) return cuda_error(e, "lam_pipeline_trace_rays scratch");
+    cudaMemsetAsync(scratch, 0, 8, st);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+    DevScene S = s->dev;
+    uint32_t* counter = scratch;
+    uint32_t* err = scratch + 1;
+    void* kargs[] = {&S, &rays, &n, &hits, &counter, &err};
+    cudaKernel_t k = mode == LAM_TRACE_ANY ? pl->handler->trace_any : pl->handler->trace_closest;
+    e = cudaLaunchKernel((const void*)k, dim3(sms * 8), dim3(TRACE_BLOCK), kargs, 0, st);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(scratch, st);
+        return cuda_error(e, "procedural trace launch");
+    }
+    uint32_t err_flags = 0;
+    cudaMemcpyAsync(&err_flags, err, 4, cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(scratch, st);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_error(e, "lam_pipeline_trace_rays");
+    if (err_flags & ERR_STACK_OVERFLOW) return set_error(LAM_ERR_STACK_OVERFLOW, "traversal stack overflow");
     return LAM_OK;
 }

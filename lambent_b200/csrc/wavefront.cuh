@@ -1,0 +1,83 @@
+// wavefront.cuh - kernel arguments of the wavefront renderer (wavefront.cu) shared with the
+// run-time-linked procedural traversal kernels (procedural.cu).
+#pragma once
+#include "device_math.cuh"
+#include "scene.h"
+#include "guide.cuh"
+
+namespace lam {
+
+constexpr int WAVE_BLOCK = 128;
+constexpr uint32_t NO_REC = 0xFFFFFFFFu;
+
+// ---------------------------------------------------------------- batched renders
+// A request of lam_batch_render: its scene, camera, image and samples.
+struct BatchReq {
+    DevScene S;
+    lam_camera cam;
+    v3 camera_pos;
+    uint32_t width, height, npix, samples, seed_offset;
+    uint32_t pix_base;  // first entry of this request's pixels in the batch's per-pixel pools
+    float4 *out_color, *out_normal, *out_albedo;
+};
+// A segment of a wave: `count` consecutive samples (from `first`) of every pixel of one request,
+// as paths path_base + s * npix + pixel.
+struct BatchSeg {
+    uint32_t req, first, count, path_base;
+    uint32_t pix_thread_base;  // first generate/accumulate thread of the segment within its wave
+};
+
+// ---------------------------------------------------------------- kernel arguments
+struct Args {
+    DevScene S;
+    lam_camera cam;
+    uint32_t width, height, npix, samples, max_depth, restir, seed_offset;
+    float tmin, tmax;
+    uint32_t wave_first, wave_count;
+    // wave buffers
+    float4 *ray_o, *ray_d;
+    uint2* hit;
+    uint32_t *q_in, *q_out;
+    uint32_t *count_in, *count_out, *work;
+    uint32_t* err;
+    unsigned long long* segments;
+    float4 *thr, *acc;
+    float* brdf;
+    uint32_t *seed, *flags;
+    float4 *ort, *orad, *ppoint, *pnormal, *vpoint, *vnormal, *lnormal, *ldir;
+    float4 *pix_color, *pix_orad, *pix_emission, *pix_albedo;
+    lam_markov_chain *tent_snap, *tent_live;
+    // data buffers
+    const lam_markov_chain* old_chains;
+    lam_markov_chain* chains;
+    uint64_t chains_len, old_chains_len;
+    uint32_t* world;
+    const uint32_t* old_world;
+    uint64_t world_len;
+    lam_reservoir* reservoirs;
+    lam_info* info;
+    uint32_t* pixel_seed;
+    // outputs
+    float4 *out_color, *out_normal, *out_albedo;
+    v3 camera_pos;
+    // learned guiding
+    uint32_t *dq, *dq_count;
+    float4 *def_n, *def_t, *def_c;
+    float* recs;             // training records (GUIDE_RECORD_STRIDE floats), null when not training
+    uint32_t rec_cap;
+    float rec_prob;          // probability that a deferred vertex is recorded
+    uint32_t *rec_count, *rec_head;
+    const uint16_t* guide_w; // packed BF16 weights
+    float guide_frac;
+    float box[6];
+    // procedural hits (run-time-linked intersection handler): per path (normal, t), (tangent, 0)
+    float4 *phit_a, *phit_b;
+    // batched renders
+    const BatchReq* reqs;
+    const BatchSeg* segs;    // this wave's segments
+    uint32_t nsegs, pix_threads;
+    uint32_t* req_done;      // per request: pixels finished
+    unsigned long long* req_time;  // per request: global timer at completion; [n] = batch start
+};
+
+}  // namespace lam

@@ -360,3 +360,20 @@ def unit_cube_scene(width=128, height=128):
     s.attributes = [solid((20, 20, 0, 255))]
     s.camera = make_camera((2.5, 2.0, 2.5), (0.5, 0.5, 0.5), 45.0, width / height)
     return s
+
+
+def with_spheres(s, n=48, seed=0, scale=0.9, angle_deg=30.0, offset=(0.1, 0.7, 0.0), material=0):
+    """Adds an instance of procedural geometry: n axis-aligned cubes, each holding the sphere inscribed
+    in it (radius = half the x extent), for an intersection handler such as tests/data/sphere_handler.cu.
+    The instance is rotated about y, scaled uniformly and moved by `offset`."""
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(-0.6, 0.6, (n, 3))
+    r = rng.uniform(0.04, 0.12, n)
+    aabbs = np.concatenate([c - r[:, None], c + r[:, None]], axis=1).astype(np.float32)
+    a = math.radians(angle_deg)
+    ca, sa = math.cos(a) * scale, math.sin(a) * scale
+    xf = np.array([ca, 0.0, sa, offset[0], 0.0, scale, 0.0, offset[1], -sa, 0.0, ca, offset[2]], np.float32)
+    s.blas.append({"aabbs": aabbs, "flags": 1})
+    s.instances.append({"transform": xf, "blas": len(s.blas) - 1,
+                        "material_indices": np.full(n, material, np.uint32)})
+    return s
