@@ -256,6 +256,15 @@ LAM_DEV bool ray_box(const TravRay& r, float4 lo, float4 hi, float tmin, float l
     return tn <= tf * 1.00000095367431640625f;
 }
 
+enum : int { STEP_MORE = 0, STEP_DONE = 1, STEP_COOP = 2 };
+
+// Per-warp shared memory of the cooperative triangle phase (one slot per lane).
+struct CoopScratch {
+    float ox[32], oy[32], oz[32], sx[32], sy[32], sz[32], tmin[32], lim[32];
+    uint32_t perm[32], excl[32], mask[32], base[32], item[32];
+    unsigned long long key[32];
+};
+
 // Alpha-test callback for non-opaque geometry: candidate accepted unless the diffuse texel's
 // alpha is near zero, transparent materials always accepted (general.wesl:1059-1067).
 LAM_DEV bool alpha_accept(const DevScene& S, uint32_t inst, uint32_t prim, float bu, float bv, bool transparent_passes);
@@ -301,11 +310,14 @@ struct Traverser {
         else err |= ERR_STACK_OVERFLOW;
     }
 
-    // Returns false once the traversal has finished (res is final).  `stack` holds
-    // TRAVERSAL_STACK entries owned by this lane (kept outside the struct so that the struct
-    // itself stays in registers).
-    LAM_DEV bool step(const DevScene& S, const uint4* __restrict__ tlas_nodes, const DevInstance* __restrict__ insts,
-                      uint2* stack, uint32_t& err) {
+    // One traversal step: one node, then the leaf items it exposes.  Returns STEP_MORE, STEP_DONE
+    // (res is final), or, with COOP, STEP_COOP when the exposed items are triangles of an opaque
+    // instance: they are left in tg for the warp's shared triangle phase (coop_triangles), after
+    // which finish_coop() completes the step.  `stack` holds TRAVERSAL_STACK entries owned by this
+    // lane (kept outside the struct so that the struct itself stays in registers).
+    template <bool COOP>
+    LAM_DEV int step_impl(const DevScene& S, const uint4* __restrict__ tlas_nodes, const DevInstance* __restrict__ insts,
+                          uint2* stack, uint32_t& err) {
         if (ng.y > 0x00FFFFFFu) {
             const uint32_t k = __ffs(ng.y >> 24) - 1u;
             ng.y &= ~(1u << (24u + k));
@@ -318,6 +330,8 @@ struct Traverser {
             tg = ng;
             ng = make_uint2(0u, 0u);
         }
+        if (COOP && blas_base >= 0 && tg.y != 0u && (cur_flags & (INST_OPAQUE | INST_PROCEDURAL)) == INST_OPAQUE)
+            return STEP_COOP;
         while (tg.y != 0u) {
             const uint32_t k = __ffs(tg.y) - 1u;
             tg.y &= tg.y - 1u;
@@ -341,7 +355,7 @@ struct Traverser {
                 setup_ray(R, oo, od);
                 ng = make_uint2(root, (1u << (24u + R.oct)) | 1u);
                 tg = make_uint2(0u, 0u);
-                return true;
+                return STEP_MORE;
             }
             const float4* tp = S.tris + 3u * item;
             if (cur_flags & INST_PROCEDURAL) {
@@ -387,7 +401,7 @@ struct Traverser {
                 res.ptg = make_float3(ai.tangent[0], ai.tangent[1], ai.tangent[2]);
                 if (ANY) {
                     res.t = best_t;
-                    return false;
+                    return STEP_DONE;
                 }
 #endif
                 continue;
@@ -411,9 +425,20 @@ struct Traverser {
             res.prim = prim;
             if (ANY) {
                 res.t = best_t;
-                return false;
+                return STEP_DONE;
             }
         }
+        return tail(stack) ? STEP_MORE : STEP_DONE;
+    }
+
+    // Returns false once the traversal has finished (res is final).
+    LAM_DEV bool step(const DevScene& S, const uint4* __restrict__ tlas_nodes, const DevInstance* __restrict__ insts,
+                      uint2* stack, uint32_t& err) {
+        return step_impl<false>(S, tlas_nodes, insts, stack, err) == STEP_MORE;
+    }
+
+    // End of a step: leave a finished instance, pop the next group; false when the ray is done.
+    LAM_DEV bool tail(uint2* stack) {
         if (ng.y <= 0x00FFFFFFu) {
             if (blas_base >= 0 && sp == blas_base) {
                 blas_base = -1;
@@ -430,6 +455,110 @@ struct Traverser {
         }
         return true;
     }
+
+    // Completes a STEP_COOP step once the warp has tested this lane's triangles.
+    LAM_DEV bool finish_coop(uint2* stack, bool hit_now) {
+        if (ANY && hit_now) {
+            res.t = best_t;
+            return false;
+        }
+        return tail(stack);
+    }
+
+    // The warp's shared triangle phase: every lane of the warp takes part.  The pending triangles
+    // (tg) of the lanes with `want` are dealt out over all 32 lanes; each tester runs the watertight
+    // test against its owner's ray and folds (t, primitive) into the owner's slot with a 64-bit
+    // shared-memory atomic minimum.  The owner then commits the minimum under the same rules as the
+    // serial loop (closest, ties to the lowest (instance, primitive)), so results are bit-identical.
+    // Returns whether this lane committed a new hit.
+    LAM_DEV bool coop_triangles(bool want, const DevScene& S, CoopScratch& ws) {
+        const uint32_t lane = threadIdx.x & 31u;
+        const uint32_t mask = want ? tg.y : 0u;
+        const uint32_t cnt = __popc(mask);
+        uint32_t incl = cnt;
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        ws.excl[lane] = incl - cnt;
+        ws.mask[lane] = mask;
+        ws.base[lane] = tg.x;
+        ws.ox[lane] = R.o.x;
+        ws.oy[lane] = R.o.y;
+        ws.oz[lane] = R.o.z;
+        ws.sx[lane] = R.Sx;
+        ws.sy[lane] = R.Sy;
+        ws.sz[lane] = R.Sz;
+        ws.perm[lane] = (uint32_t)R.kx | ((uint32_t)R.ky << 2) | ((uint32_t)R.kz << 4);
+        ws.tmin[lane] = tmin;
+        ws.lim[lane] = best_t;
+        ws.key[lane] = ~0ull;
+        __syncwarp();
+        for (uint32_t c0 = 0; c0 < total; c0 += 32u) {
+            const uint32_t j = c0 + lane;
+            bool has = false;
+            unsigned long long key = 0ull;
+            uint32_t owner = 0u, item = 0u;
+            if (j < total) {
+                // owner of test j: the last lane whose exclusive count is <= j
+                uint32_t lo = 0u, hi = 31u;
+#pragma unroll
+                for (int it = 0; it < 5; ++it) {
+                    const uint32_t mid = (lo + hi + 1u) >> 1;
+                    if (ws.excl[mid] <= j) lo = mid;
+                    else hi = mid - 1u;
+                }
+                owner = lo;
+                const uint32_t bit = __fns(ws.mask[owner], 0u, (int)(j - ws.excl[owner]) + 1);
+                item = ws.base[owner] + bit;
+                TravRay r;
+                r.o = make_float3(ws.ox[owner], ws.oy[owner], ws.oz[owner]);
+                r.Sx = ws.sx[owner];
+                r.Sy = ws.sy[owner];
+                r.Sz = ws.sz[owner];
+                const uint32_t pm = ws.perm[owner];
+                r.kx = (int)(pm & 3u);
+                r.ky = (int)((pm >> 2) & 3u);
+                r.kz = (int)((pm >> 4) & 3u);
+                const float4* tp = S.tris + 3u * item;
+                const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                float t;
+                if (wbw_f32(r, a, b, c, ws.lim[owner], &t) && t > ws.tmin[owner]) {
+                    const uint32_t u = __float_as_uint(t);
+                    const uint32_t ord = (u & 0x80000000u) ? ~u : (u | 0x80000000u);  // float order as unsigned
+                    key = ((unsigned long long)ord << 32) | __float_as_uint(a.w);
+                    atomicMin(&ws.key[owner], key);
+                    has = true;
+                }
+            }
+            __syncwarp();
+            if (has && key == ws.key[owner]) ws.item[owner] = item;  // (t, primitive) names one triangle
+            __syncwarp();
+        }
+        bool hit_now = false;
+        if (want) {
+            const unsigned long long key = ws.key[lane];
+            if (key != ~0ull) {
+                const uint32_t ord = (uint32_t)(key >> 32);
+                const float t = __uint_as_float((ord & 0x80000000u) ? (ord & 0x7FFFFFFFu) : ~ord);
+                const uint32_t prim = (uint32_t)key;
+                const bool better = t < best_t || (t == best_t && res.tri != NO_HIT &&
+                                                   (cur_inst < res.inst || (cur_inst == res.inst && prim < res.prim)));
+                if (better) {
+                    best_t = t;
+                    res.tri = ws.item[lane];
+                    res.inst = cur_inst;
+                    res.prim = prim;
+                    hit_now = true;
+                }
+            }
+            tg.y = 0u;
+        }
+        __syncwarp();
+        return hit_now;
+    }
 };
 
 // Lanes below this many active rays trigger a refill of the idle lanes from the work queue.
@@ -439,12 +568,17 @@ struct Traverser {
 constexpr int REFILL_THRESHOLD = LAM_REFILL_THRESHOLD;
 
 // Persistent warp loop over work items [0, n) claimed with a global counter.  `load(i, o, d, t0, t1)`
-// fetches item i; `store(i, res)` consumes a finished traversal.  Every lane of the warp must call it.
+// fetches item i; `store(i, res)` consumes a finished traversal.  Every lane of the warp must call it,
+// in blocks of 128 threads.  Triangle tests of opaque instances are dealt out over the whole warp
+// (Traverser::coop_triangles): with one ray per lane, a step exposes 0 to 24 triangles per lane, and
+// a per-lane loop would run as long as the busiest lane.
 template <bool ANY, bool ALPHA, class Load, class Store>
 LAM_DEV void trace_persistent(const DevScene& S, const uint4* __restrict__ tl, const DevInstance* __restrict__ in,
                               uint32_t n, uint32_t* __restrict__ work, uint32_t& err, Load load, Store store) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
+    __shared__ CoopScratch coop_ws[4];  // one per warp of a 128-thread block
+    CoopScratch& ws = coop_ws[(threadIdx.x >> 5) & 3u];
     Traverser<ANY, ALPHA> T;
     uint2 stack[TRAVERSAL_STACK];
     bool active = false, exhausted = false;
@@ -471,7 +605,14 @@ LAM_DEV void trace_persistent(const DevScene& S, const uint4* __restrict__ tl, c
             if (base + (uint32_t)__popc(need) >= n) exhausted = true;
         }
         if (!__any_sync(0xFFFFFFFFu, active)) break;
-        if (active && !T.step(S, tl, in, stack, err)) {
+        int code = STEP_MORE;
+        if (active) code = T.template step_impl<true>(S, tl, in, stack, err);
+        const bool want = active && code == STEP_COOP;
+        if (__any_sync(0xFFFFFFFFu, want)) {  // warp-uniform: triangle tests dealt out over all lanes
+            const bool hit_now = T.coop_triangles(want, S, ws);
+            if (want) code = T.finish_coop(stack, hit_now) ? STEP_MORE : STEP_DONE;
+        }
+        if (active && code == STEP_DONE) {
             store(item, T.res);
             active = false;
         }
