@@ -263,6 +263,7 @@ struct CoopScratch {
     float ox[32], oy[32], oz[32], sx[32], sy[32], sz[32], tmin[32], lim[32];
     uint32_t perm[32], excl[32], mask[32], base[32], item[32];
     unsigned long long key[32];
+    const float4* tris[32];  // the owner's triangle array (lanes of one warp may trace different scenes)
 };
 
 // Alpha-test callback for non-opaque geometry: candidate accepted unless the diffuse texel's
@@ -472,6 +473,9 @@ struct Traverser {
     // serial loop (closest, ties to the lowest (instance, primitive)), so results are bit-identical.
     // Returns whether this lane committed a new hit.
     LAM_DEV bool coop_triangles(bool want, const DevScene& S, CoopScratch& ws) {
+        return coop_triangles_from(want, S.tris, ws);
+    }
+    LAM_DEV bool coop_triangles_from(bool want, const float4* my_tris, CoopScratch& ws) {
         const uint32_t lane = threadIdx.x & 31u;
         const uint32_t mask = want ? tg.y : 0u;
         const uint32_t cnt = __popc(mask);
@@ -495,6 +499,7 @@ struct Traverser {
         ws.tmin[lane] = tmin;
         ws.lim[lane] = best_t;
         ws.key[lane] = ~0ull;
+        ws.tris[lane] = my_tris;
         __syncwarp();
         for (uint32_t c0 = 0; c0 < total; c0 += 32u) {
             const uint32_t j = c0 + lane;
@@ -522,7 +527,7 @@ struct Traverser {
                 r.kx = (int)(pm & 3u);
                 r.ky = (int)((pm >> 2) & 3u);
                 r.kz = (int)((pm >> 4) & 3u);
-                const float4* tp = S.tris + 3u * item;
+                const float4* tp = ws.tris[owner] + 3u * item;
                 const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
                 float t;
                 if (wbw_f32(r, a, b, c, ws.lim[owner], &t) && t > ws.tmin[owner]) {
@@ -625,6 +630,8 @@ template <bool ANY, bool ALPHA, class Load, class Store>
 LAM_DEV void trace_persistent_multi(uint32_t n, uint32_t* __restrict__ work, uint32_t& err, Load load, Store store) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
+    __shared__ CoopScratch coop_ws[4];  // one per warp of a 128-thread block
+    CoopScratch& ws = coop_ws[(threadIdx.x >> 5) & 3u];
     Traverser<ANY, ALPHA> T;
     uint2 stack[TRAVERSAL_STACK];
     const DevScene* sp = nullptr;
@@ -652,7 +659,14 @@ LAM_DEV void trace_persistent_multi(uint32_t n, uint32_t* __restrict__ work, uin
             if (base + (uint32_t)__popc(need) >= n) exhausted = true;
         }
         if (!__any_sync(0xFFFFFFFFu, active)) break;
-        if (active && !T.step(*sp, sp->tlas_nodes, sp->inst, stack, err)) {
+        int code = STEP_MORE;
+        if (active) code = T.template step_impl<true>(*sp, sp->tlas_nodes, sp->inst, stack, err);
+        const bool want = active && code == STEP_COOP;
+        if (__any_sync(0xFFFFFFFFu, want)) {
+            const bool hit_now = T.coop_triangles_from(want, want ? sp->tris : nullptr, ws);
+            if (want) code = T.finish_coop(stack, hit_now) ? STEP_MORE : STEP_DONE;
+        }
+        if (active && code == STEP_DONE) {
             store(item, T.res);
             active = false;
         }
