@@ -28,6 +28,10 @@ sys.path.insert(0, ROOT)
 METRIC = "Mrays/s at 1080p/1.3M tris"
 SEG_BYTES_EXTEND = 48   # ray (o, d, tmax) 28 B read + hit 20 B write per segment
 SEG_BYTES_TOTAL = 280   # extend 48 + shade 232 (compulsory wavefront traffic per segment)
+# DRAM bytes (read + write) per segment of the extend kernel, from one ncu capture of all extend
+# launches of a 960x540, 4-spp render of the same scene (profiles/extend_kernel_icosphere_field_960x540.md);
+# traffic grows with the segments processed, so a full launch's traffic is this times its segments.
+EXTEND_DRAM_BYTES_PER_SEGMENT = 188.0
 
 
 def parse():
@@ -540,7 +544,10 @@ def run_ours(a):
             "roofline": {"bound": "hbm", "kernel": "extend_kernel (BVH8 traversal)",
                          "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 5), "peak_kind": f"{peak_kind} hbm_gbs",
-                         "bytes_per_segment": SEG_BYTES_EXTEND, "traffic": None,
+                         "bytes_per_segment": SEG_BYTES_EXTEND,
+                         "traffic": round(EXTEND_DRAM_BYTES_PER_SEGMENT * segs / max(1, prof.extend_launches)),
+                         "traffic_note": "DRAM bytes per extend launch: ncu bytes/segment of a 960x540 capture x this "
+                                         "run's segments per launch (BVH and triangle fetches that miss L2)",
                          "extend_ms": round(prof.extend_ms, 3), "shade_ms": round(prof.shade_ms, 3),
                          "generate_ms": round(prof.generate_ms, 3), "accumulate_ms": round(prof.accumulate_ms, 3),
                          "shade_gbs": round(shade_gbs, 2)},
