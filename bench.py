@@ -140,23 +140,23 @@ def cpu_reference(a, scene, seconds):
     from lambent_b200 import _abi
     cores = os.cpu_count() or 1
     osc = O.OracleScene(scene)
-    x0, y0 = a.width // 2 - 32, a.height // 2 - 32
-    w = h = 64
+    w = h = min(128, min(a.width, a.height)) // 32 * 32  # calibration crop
+    x0, y0 = a.width // 2 - w // 2, a.height // 2 - h // 2
     spp = 2
     t0 = time.perf_counter()
     r = osc.render(scene.camera, a.width, a.height, samples=spp, max_depth=a.depth, restir=_abi.RESTIR_DISABLED,
                    crop=(x0, y0, w, h), threads=cores)
     dt = time.perf_counter() - t0
-    # grow the crop towards the time budget (square, centred), keep at least one calibration run
-    scale = max(1.0, min(64.0, seconds / max(dt, 1e-3)))
-    side = int(min(min(a.width, a.height), 64 * scale ** 0.5)) // 32 * 32
-    if side > 64:
-        x0, y0 = a.width // 2 - side // 2, a.height // 2 - side // 2
-        t0 = time.perf_counter()
-        r = osc.render(scene.camera, a.width, a.height, samples=spp, max_depth=a.depth, restir=_abi.RESTIR_DISABLED,
-                       crop=(x0, y0, side, side), threads=cores)
-        dt = time.perf_counter() - t0
-        w = h = side
+    # fill the time budget: the largest centre crop up to 1024^2, then as many samples as fit
+    side = min(1024, min(a.width, a.height)) // 32 * 32
+    per_px = dt / (w * h * spp)  # seconds per pixel-sample at the calibration size
+    spp = int(max(1, min(64, round(seconds / max(per_px * side * side, 1e-9)))))
+    x0, y0 = a.width // 2 - side // 2, a.height // 2 - side // 2
+    t0 = time.perf_counter()
+    r = osc.render(scene.camera, a.width, a.height, samples=spp, max_depth=a.depth, restir=_abi.RESTIR_DISABLED,
+                   crop=(x0, y0, side, side), threads=cores)
+    dt = time.perf_counter() - t0
+    w = h = side
     mrays = r["segments"] / dt / 1e6
     return {"value": round(mrays, 3), "unit": "Mrays/s", "cores": cores, "kind": "port",
             "sample": f"centre crop {w}x{h} of the {a.width}x{a.height} frame, {spp} spp, depth {a.depth}, "
