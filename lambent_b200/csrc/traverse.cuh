@@ -179,16 +179,9 @@ LAM_DEV float qbyte(uint32_t w, uint32_t k) {
 
 // Intersects the 8 children of one node.  Outputs the node group (child_base, internal hits in
 // bits 24..31 in octant order | imask) and the leaf group (leaf_base, item hits in bits 0..23).
-template <bool GLOBAL>
-LAM_DEV uint4 load_node_word(const uint4* p) {
-    return *p;
-}
-
-template <bool GLOBAL = false>
 LAM_DEV void intersect_node(const uint4* __restrict__ np, const TravRay& r, float tmin, float tmax, uint2& ng,
                             uint2& tg) {
-    const uint4 n0 = load_node_word<GLOBAL>(np), n1 = load_node_word<GLOBAL>(np + 1), n2 = load_node_word<GLOBAL>(np + 2),
-                n3 = load_node_word<GLOBAL>(np + 3), n4 = load_node_word<GLOBAL>(np + 4);
+    const uint4 n0 = np[0], n1 = np[1], n2 = np[2], n3 = np[3], n4 = np[4];
     const float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
     const uint32_t imask = n0.w >> 24;
     const float sx = __uint_as_float((n0.w & 0xFFu) << 23);
@@ -325,8 +318,9 @@ struct Traverser {
             const uint32_t slot = k ^ R.oct;
             const uint32_t child = ng.x + __popc(ng.y & ((1u << slot) - 1u) & 0xFFu);
             if (ng.y > 0x00FFFFFFu) push(stack, ng, err);
-            if (blas_base < 0) intersect_node<false>(tlas_nodes + 5u * child, R, tmin, best_t, ng, tg);
-            else intersect_node<true>(S.blas_nodes + 5u * child, R, tmin, best_t, ng, tg);
+            // one call site for TLAS and BLAS nodes: lanes of a warp on either level share one test
+            // (two call sites run the 8-wide test twice whenever a warp straddles the levels)
+            intersect_node((blas_base < 0 ? tlas_nodes : S.blas_nodes) + 5u * child, R, tmin, best_t, ng, tg);
         } else {
             tg = ng;
             ng = make_uint2(0u, 0u);
