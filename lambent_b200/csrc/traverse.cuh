@@ -172,9 +172,10 @@ LAM_DEV void wbw_f64(float3 of, float3 df, float4 p0, float4 p1, float4 p2, floa
     *front = nd < 0.0;
 }
 
-// One quantized child coordinate as an exact float (byte k of w).
-LAM_DEV float qbyte(uint32_t w, uint32_t k) {
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + k)) - 8388608.0f;
+// Byte k of w as the float 1 + byte * 2^-15 (the byte in mantissa bits 8..15 of 1.0f): one byte
+// permute turns a quantized child coordinate into an exact float.
+LAM_DEV float qone(uint32_t w, uint32_t k) {
+    return __uint_as_float(__byte_perm(w, 0x3F800000u, 0x7604u + (k << 4)));
 }
 
 // Intersects the 8 children of one node.  Outputs the node group (child_base, internal hits in
@@ -197,15 +198,23 @@ LAM_DEV void intersect_node(const uint4* __restrict__ np, const TravRay& r, floa
     const uint32_t ny0 = fy ? n4.x : n2.z, ny1 = fy ? n4.y : n2.w, fy0 = fy ? n2.z : n4.x, fy1 = fy ? n2.w : n4.y;
     const uint32_t nz0 = fz ? n4.z : n3.x, nz1 = fz ? n4.w : n3.y, fz0 = fz ? n3.x : n4.z, fz1 = fz ? n3.y : n4.w;
     uint32_t node_hits = 0u, leaf_hits = 0u;
+    // t = q * adx + aox with q read as 1 + q * 2^-15: t = (1 + q * 2^-15) * (2^15 adx) + (aox - 2^15 adx).
+    // Rounding B adds at most 2^-9 of a grid step (plus 2^-24 |aox|) to each plane distance, far inside
+    // the builder's one-step outward padding and the 2^-20 far-plane margin.  This saves the
+    // subtraction of an integer-to-float conversion per plane.  Should 2^15 adx overflow, the plane
+    // distance is NaN, which fmaxf / fminf ignore: the test only becomes more permissive.
+    const float Ax = 32768.0f * adx, Ay = 32768.0f * ady, Az = 32768.0f * adz;
+    const float Bx = __fmaf_rn(-32768.0f, adx, aox), By = __fmaf_rn(-32768.0f, ady, aoy),
+                Bz = __fmaf_rn(-32768.0f, adz, aoz);
 #pragma unroll
     for (uint32_t i = 0; i < 8; ++i) {
         const uint32_t k = i & 3u;
-        const float tnx = __fmaf_rn(qbyte(i < 4 ? nx0 : nx1, k), adx, aox);
-        const float tny = __fmaf_rn(qbyte(i < 4 ? ny0 : ny1, k), ady, aoy);
-        const float tnz = __fmaf_rn(qbyte(i < 4 ? nz0 : nz1, k), adz, aoz);
-        const float tfx = __fmaf_rn(qbyte(i < 4 ? fx0 : fx1, k), adx, aox);
-        const float tfy = __fmaf_rn(qbyte(i < 4 ? fy0 : fy1, k), ady, aoy);
-        const float tfz = __fmaf_rn(qbyte(i < 4 ? fz0 : fz1, k), adz, aoz);
+        const float tnx = __fmaf_rn(qone(i < 4 ? nx0 : nx1, k), Ax, Bx);
+        const float tny = __fmaf_rn(qone(i < 4 ? ny0 : ny1, k), Ay, By);
+        const float tnz = __fmaf_rn(qone(i < 4 ? nz0 : nz1, k), Az, Bz);
+        const float tfx = __fmaf_rn(qone(i < 4 ? fx0 : fx1, k), Ax, Bx);
+        const float tfy = __fmaf_rn(qone(i < 4 ? fy0 : fy1, k), Ay, By);
+        const float tfz = __fmaf_rn(qone(i < 4 ? fz0 : fz1, k), Az, Bz);
         const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
         const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
         if (tn <= tf * 1.00000095367431640625f) {
