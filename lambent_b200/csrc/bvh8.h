@@ -12,8 +12,10 @@
 // Child box of slot i on axis a: [p_a + qlo_a[i] * 2^(e_a-127), p_a + qhi_a[i] * 2^(e_a-127)],
 // padded outward by one grid step so the box test stays conservative under f32 rounding.
 // imask bit i: slot i is an internal child; its node index is child_base + popc(imask & ((1<<i)-1)).
-// meta[i] for a leaf slot: (count << 5) | offset, items leaf_base + offset .. + count - 1 (count 1..3);
-// meta[i] == 0 and imask bit clear: empty slot.
+// meta[i]: bits 5..7 the slot's hit-mask bits in unary, bits 0..4 their position in the mask.
+//   leaf slot: ((1 << count) - 1) << 5 | offset, items leaf_base + offset .. + count - 1 (count 1..3);
+//   internal slot: 1 << 5 | (24 + i) (a ray of octant o sets bit 24 + (i ^ o));
+//   empty slot: 0 (imask bit clear).
 // Slots are assigned so that slot o holds the child a ray of octant o (sign bits x|y<<1|z<<2 of
 // its direction) should visit first; traversal visits slot (k ^ octant) for k = 0..7.
 #pragma once

@@ -318,11 +318,12 @@ void build_bvh8(const float* boxes, uint32_t n, int max_leaf, Bvh8* out) {
             cboxes[s] = c.box;
             used[s] = true;
             if (ch_leaf[i]) {
-                nd.meta[s] = (uint8_t)((c.count << 5) | leaf_off);
+                nd.meta[s] = (uint8_t)((((1u << c.count) - 1u) << 5) | leaf_off);
                 for (uint32_t k = 0; k < c.count; ++k) out->leaf_items.push_back(b2.items[c.first + k]);
                 leaf_off += c.count;
             } else {
                 nd.imask |= (uint8_t)(1u << s);
+                nd.meta[s] = (uint8_t)((1u << 5) | (24u + s));
                 new_children.push_back({ch[i], next_child++});
             }
         }

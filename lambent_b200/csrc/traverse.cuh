@@ -197,7 +197,15 @@ LAM_DEV void intersect_node(const uint4* __restrict__ np, const TravRay& r, floa
     const uint32_t nx0 = fx ? n3.z : n2.x, nx1 = fx ? n3.w : n2.y, fx0 = fx ? n2.x : n3.z, fx1 = fx ? n2.y : n3.w;
     const uint32_t ny0 = fy ? n4.x : n2.z, ny1 = fy ? n4.y : n2.w, fy0 = fy ? n2.z : n4.x, fy1 = fy ? n2.w : n4.y;
     const uint32_t nz0 = fz ? n4.z : n3.x, nz1 = fz ? n4.w : n3.y, fz0 = fz ? n3.x : n4.z, fz1 = fz ? n3.y : n4.w;
-    uint32_t node_hits = 0u, leaf_hits = 0u;
+    // Hit-mask contribution of each slot, four slots per word: bits (bits 5..7 of meta, unary) at
+    // position `at` (bits 0..4; internal children sit at 24 + slot, which is XORed with the octant).
+    // A byte is internal when its position is 24..31 (bits 3 and 4 set); bit 0 of each byte of
+    // inner_* flags it, so inner_* * oct holds the octant in exactly the internal bytes.
+    const uint32_t ma = n1.z, mb = n1.w;
+    const uint32_t inner_a = ((ma & (ma << 1)) >> 4) & 0x01010101u, inner_b = ((mb & (mb << 1)) >> 4) & 0x01010101u;
+    const uint32_t at_a = (ma ^ (inner_a * r.oct)) & 0x1F1F1F1Fu, at_b = (mb ^ (inner_b * r.oct)) & 0x1F1F1F1Fu;
+    const uint32_t bits_a = (ma >> 5) & 0x07070707u, bits_b = (mb >> 5) & 0x07070707u;
+    uint32_t hits = 0u;
     // t = q * adx + aox with q read as 1 + q * 2^-15: t = (1 + q * 2^-15) * (2^15 adx) + (aox - 2^15 adx).
     // Rounding B adds at most 2^-9 of a grid step (plus 2^-24 |aox|) to each plane distance, far inside
     // the builder's one-step outward padding and the 2^-20 far-plane margin.  This saves the
@@ -217,17 +225,11 @@ LAM_DEV void intersect_node(const uint4* __restrict__ np, const TravRay& r, floa
         const float tfz = __fmaf_rn(qone(i < 4 ? fz0 : fz1, k), Az, Bz);
         const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
         const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
-        if (tn <= tf * 1.00000095367431640625f) {
-            const uint32_t meta = ((i < 4 ? n1.z : n1.w) >> (8u * k)) & 0xFFu;
-            if (imask & (1u << i)) {
-                node_hits |= 1u << (i ^ r.oct);
-            } else {
-                leaf_hits |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
-            }
-        }
+        if (tn <= tf * 1.00000095367431640625f)
+            hits |= __byte_perm(i < 4 ? bits_a : bits_b, 0u, 0x4440u + k) << __byte_perm(i < 4 ? at_a : at_b, 0u, 0x4440u + k);
     }
-    ng = make_uint2(n1.x, (node_hits << 24) | imask);
-    tg = make_uint2(n1.y, leaf_hits);
+    ng = make_uint2(n1.x, (hits & 0xFF000000u) | imask);
+    tg = make_uint2(n1.y, hits & 0x00FFFFFFu);
 }
 
 struct TraceResult {
