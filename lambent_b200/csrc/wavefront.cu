@@ -393,7 +393,11 @@ LAM_DEV void finalize_records(const Args& A, uint32_t path, v3 scol) {
 }
 
 template <int Q, bool GUIDE, bool LEARN, bool BATCH>
-__global__ void __launch_bounds__(WAVE_BLOCK) shade_kernel(const __grid_constant__ Args A) {
+// Six CTAs per SM for the unguided forms: the kernel waits on chains of dependent gathers (queue ->
+// hit -> triangle -> material -> texture), so resident warps matter more than the few registers
+// that spill (measured: 79 ms against 87 ms per 16-spp step at 1080p).  The Markov-guided form keeps
+// its registers (213 unbounded; 1 KB of spill at 80).
+__global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(const __grid_constant__ Args A) {
     const uint32_t n = *A.count_in;
     const uint32_t lane = threadIdx.x & 31u;
     Grid G;
