@@ -56,12 +56,14 @@ LAM_DEV void setup_ray(TravRay& r, float3 o, float3 d) {
     float dz = sel3(kz, d.x, d.y, d.z);
     if (dz < 0.0f) { int t = kx; kx = ky; ky = t; }
     r.kx = kx; r.ky = ky; r.kz = kz;
-    r.Sx = __fdiv_rn(sel3(kx, d.x, d.y, d.z), dz);
-    r.Sy = __fdiv_rn(sel3(ky, d.x, d.y, d.z), dz);
+    // shear constants from one IEEE reciprocal (the oracle uses the same three operations); any
+    // constants serve, as long as every triangle a ray meets is tested with the same ones
     r.Sz = __fdiv_rn(1.0f, dz);
+    r.Sx = __fmul_rn(sel3(kx, d.x, d.y, d.z), r.Sz);
+    r.Sy = __fmul_rn(sel3(ky, d.x, d.y, d.z), r.Sz);
 }
 
-// setup_ray without the three divisions of the shear constants (restores a ray whose Sx, Sy, Sz
+// setup_ray without the reciprocal and products of the shear constants (restores a ray whose Sx, Sy, Sz
 // are known).
 LAM_DEV void setup_ray_keep_shear(TravRay& r, float3 o, float3 d) {
     r.o = o;
@@ -258,6 +260,20 @@ LAM_DEV bool ray_box(const TravRay& r, float4 lo, float4 hi, float tmin, float l
     const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
     const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), limit));
     return tn <= tf * 1.00000095367431640625f;
+}
+
+// Position of the r-th (from 0) set bit of m; r < popc(m).  Four population counts of halving
+// windows (cheaper here than __fns).
+LAM_DEV uint32_t nth_set_bit(uint32_t m, uint32_t r) {
+    uint32_t pos = 0u, c = __popc(m & 0xFFFFu);
+    if (r >= c) { r -= c; m >>= 16; pos += 16u; }
+    c = __popc(m & 0xFFu);
+    if (r >= c) { r -= c; m >>= 8; pos += 8u; }
+    c = __popc(m & 0xFu);
+    if (r >= c) { r -= c; m >>= 4; pos += 4u; }
+    c = __popc(m & 0x3u);
+    if (r >= c) { r -= c; m >>= 2; pos += 2u; }
+    return pos + ((r >= (m & 1u)) ? 1u : 0u);
 }
 
 enum : int { STEP_MORE = 0, STEP_DONE = 1, STEP_COOP = 2 };
@@ -521,7 +537,7 @@ struct Traverser {
                     else hi = mid - 1u;
                 }
                 owner = lo;
-                const uint32_t bit = __fns(ws.mask[owner], 0u, (int)(j - ws.excl[owner]) + 1);
+                const uint32_t bit = nth_set_bit(ws.mask[owner], j - ws.excl[owner]);
                 item = ws.base[owner] + bit;
                 TravRay r;
                 r.o = make_float3(ws.ox[owner], ws.oy[owner], ws.oz[owner]);

@@ -53,9 +53,10 @@ WbwRay wbw_setup(vec3 d) {
     if (d[kz] < 0.0f) std::swap(kx, ky);
     WbwRay r;
     r.kx = kx; r.ky = ky; r.kz = kz;
-    r.Sx = d[kx] / d[kz];
-    r.Sy = d[ky] / d[kz];
+    // one IEEE reciprocal, then two products (lambent_b200/csrc/traverse.cuh setup_ray does the same)
     r.Sz = 1.0f / d[kz];
+    r.Sx = d[kx] * r.Sz;
+    r.Sy = d[ky] * r.Sz;
     return r;
 }
 
