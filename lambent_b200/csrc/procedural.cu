@@ -34,9 +34,9 @@ extern "C" __global__ void __launch_bounds__(WAVE_BLOCK) lam_proc_extend(const _
             t1 = A.tmax;
         },
         [&](uint32_t i, const TraceResult& tr) {
-            const uint32_t path = A.q_in[i];
-            A.hit[path] = make_uint2(tr.tri, tr.inst);
+            A.hit[i] = make_uint2(tr.tri, tr.inst);
             if (tr.tri != NO_HIT && (in[tr.inst].flags & INST_PROCEDURAL)) {
+                const uint32_t path = A.q_in[i];
                 A.phit_a[path] = make_float4(tr.pn.x, tr.pn.y, tr.pn.z, tr.t);
                 A.phit_b[path] = make_float4(tr.ptg.x, tr.ptg.y, tr.ptg.z, 0.0f);
             }

@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK) extend_kernel(Args A) {
             t0 = A.tmin;
             t1 = A.tmax;
         },
-        [&](uint32_t i, const TraceResult& tr) { A.hit[A.q_in[i]] = make_uint2(tr.tri, tr.inst); });
+        [&](uint32_t i, const TraceResult& tr) { A.hit[i] = make_uint2(tr.tri, tr.inst); });
     if (err) atomicOr(A.err, err);
 }
 
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 last_dir = mk(b.x, b.y, b.z);
             }
             MC tentative = GUIDE ? mc_load(A.tent_live + pixel) : mc_zero();
-            const uint2 h = A.hit[path];
+            const uint2 h = A.hit[i];  // hits are stored by queue position (extend shares this queue)
             bool terminated = false;
             if (h.x != NO_HIT) {
                 Isect is;
@@ -1260,7 +1260,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK) extend_batch_kernel(const __grid_c
             t1 = A.tmax;
             sp = &A.reqs[A.segs[A.flags[path] >> 16].req].S;
         },
-        [&](uint32_t i, const TraceResult& tr) { A.hit[A.q_in[i]] = make_uint2(tr.tri, tr.inst); });
+        [&](uint32_t i, const TraceResult& tr) { A.hit[i] = make_uint2(tr.tri, tr.inst); });
     if (err) atomicOr(A.err, err);
 }
 

@@ -36,7 +36,7 @@ struct Args {
     uint32_t wave_first, wave_count;
     // wave buffers
     float4 *ray_o, *ray_d;
-    uint2* hit;
+    uint2* hit;  // (triangle slot, instance) of the closest hit, by position in the current queue
     uint32_t *q_in, *q_out;
     uint32_t *count_in, *count_out, *work;
     uint32_t* err;
