@@ -26,8 +26,7 @@ extern "C" __global__ void __launch_bounds__(WAVE_BLOCK) lam_proc_extend(const _
     trace_persistent<false, true>(
         A.S, tl, in, n, A.work, err,
         [&](uint32_t i, float3& o, float3& d, float& t0, float& t1) {
-            const uint32_t path = A.q_in[i];
-            const float4 o4 = A.ray_o[path], d4 = A.ray_d[path];
+            const float4 o4 = A.ray_o[i], d4 = A.ray_d[i];
             o = make_float3(o4.x, o4.y, o4.z);
             d = make_float3(d4.x, d4.y, d4.z);
             t0 = A.tmin;

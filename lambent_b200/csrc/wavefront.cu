@@ -168,7 +168,7 @@ struct WaveBuffers {
     uint32_t width = 0, height = 0, npix = 0, spp_wave = 0;
     uint64_t paths = 0;
     bool full = false, guide = false;
-    float4 *ray_o = nullptr, *ray_d = nullptr;
+    float4 *ray_o = nullptr, *ray_d = nullptr, *ray_o2 = nullptr, *ray_d2 = nullptr;  // two queues' rays
     uint2* hit = nullptr;
     uint32_t *queue0 = nullptr, *queue1 = nullptr;
     float4 *thr = nullptr, *acc = nullptr;
@@ -183,7 +183,7 @@ struct WaveBuffers {
     // learned guiding: deferred diffuse vertices and the per-path training-record lists
     bool learned = false;
     uint32_t* dq = nullptr;
-    float4 *def_n = nullptr, *def_t = nullptr, *def_c = nullptr;
+    float4 *def_n = nullptr, *def_t = nullptr, *def_c = nullptr, *def_o = nullptr, *def_d = nullptr;
     uint32_t* rec_head = nullptr;
     float4 *phit_a = nullptr, *phit_b = nullptr;  // procedural hits (allocated on first use)
     uint32_t* ctr = nullptr;  // [0..1] queue counts, [2..3] work counters, [4] error flags,
@@ -305,8 +305,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK) extend_kernel(Args A) {
     trace_persistent<false, ALPHA>(
         A.S, tl, in, n, A.work, err,
         [&](uint32_t i, float3& o, float3& d, float& t0, float& t1) {
-            const uint32_t path = A.q_in[i];
-            const float4 o4 = A.ray_o[path], d4 = A.ray_d[path];
+            const float4 o4 = A.ray_o[i], d4 = A.ray_d[i];
             o = make_float3(o4.x, o4.y, o4.z);
             d = make_float3(d4.x, d4.y, d4.z);
             t0 = A.tmin;
@@ -411,6 +410,8 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
         const uint32_t i = base + lane;
         bool cont = false, deferred = false;
         uint32_t path = 0;
+        v3 ro = splat(0.0f), rd = splat(0.0f);  // the outgoing ray once the bounce is shaded
+        float seg_w = 0.0f;                     // a batched path's segment, carried in the ray's w
         if (i < n) {
             path = A.q_in[i];
             uint32_t fl = A.flags[path];
@@ -436,8 +437,10 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
             const bool last_sample = sample_index + 1u == samples;
             const uint32_t depth = fl & 0xFFu;
             bool last_not_vmf = (fl >> 8) & 1u;
-            const float4 o4 = A.ray_o[path], d4 = A.ray_d[path];
-            v3 ro = mk(o4.x, o4.y, o4.z), rd = mk(d4.x, d4.y, d4.z);
+            const float4 o4 = A.ray_o[i], d4 = A.ray_d[i];
+            ro = mk(o4.x, o4.y, o4.z);
+            rd = mk(d4.x, d4.y, d4.z);
+            seg_w = o4.w;
             float4 th = A.thr[path];
             v3 color = mk(th.x, th.y, th.z);
             float picked = th.w;
@@ -696,8 +699,10 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 A.brdf[path] = cached_brdf;
                 A.seed[path] = seed;
                 A.flags[path] = (fl & 0xFFFF0000u) | (depth + 1u) | (last_not_vmf ? 0x100u : 0u);
-                A.ray_o[path] = make_float4(ro.x, ro.y, ro.z, 0.0f);
-                A.ray_d[path] = make_float4(rd.x, rd.y, rd.z, 0.0f);
+                if (deferred) {
+                    A.def_o[path] = make_float4(ro.x, ro.y, ro.z, 0.0f);
+                    A.def_d[path] = make_float4(rd.x, rd.y, rd.z, 0.0f);
+                }
             }
             if (rec) {
                 A.ort[path] = make_float4(orc.x, orc.y, orc.z, sum_mc);
@@ -718,7 +723,12 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
             uint32_t slot = 0;
             if (lane == 0) slot = atomicAdd(A.count_out, __popc(mask));
             slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
-            if (next) A.q_out[slot + __popc(mask & ((1u << lane) - 1u))] = path;
+            if (next) {
+                const uint32_t s = slot + __popc(mask & ((1u << lane) - 1u));
+                A.q_out[s] = path;
+                A.ray_o_out[s] = make_float4(ro.x, ro.y, ro.z, seg_w);
+                A.ray_d_out[s] = make_float4(rd.x, rd.y, rd.z, 0.0f);
+            }
         }
         if (LEARN) {
             const uint32_t dmask = __ballot_sync(0xFFFFFFFFu, deferred);
@@ -741,7 +751,7 @@ constexpr uint32_t GUIDE_TMEM_COLS = 128;  // accumulators of tiles A (columns 0
 
 template <int Q, bool NET>
 LAM_DEV void guide_finish(const Args& A, uint32_t path, const net::Lobes* L, bool& out) {
-    const float4 o4 = A.ray_o[path], d4 = A.ray_d[path], dn = A.def_n[path], dt = A.def_t[path], dc = A.def_c[path];
+    const float4 o4 = A.def_o[path], d4 = A.def_d[path], dn = A.def_n[path], dt = A.def_t[path], dc = A.def_c[path];
     const float4 th = A.thr[path], ac = A.acc[path];
     const v3 ro = mk(o4.x, o4.y, o4.z), rd = mk(d4.x, d4.y, d4.z), n = mk(dn.x, dn.y, dn.z), t = mk(dt.x, dt.y, dt.z);
     const uint32_t seed0 = __float_as_uint(dt.w);
@@ -772,7 +782,7 @@ LAM_DEV void guide_finish(const Args& A, uint32_t path, const net::Lobes* L, boo
     A.thr[path] = make_float4(color.x, color.y, color.z, th.w);
     A.brdf[path] = cached_brdf;
     A.acc[path] = make_float4(ac.x, ac.y, ac.z, pdf);
-    A.ray_d[path] = make_float4(dir.x, dir.y, dir.z, 0.0f);
+    A.def_d[path] = make_float4(dir.x, dir.y, dir.z, 0.0f);
     // a Bernoulli subset of the vertices (probability rec_prob), so that the record buffer samples every
     // pixel and depth of the wave instead of filling up with the first vertices shaded
     if (A.recs && rand_f32(rand_u32(seed0 ^ 0x2C1B3C6Du)) < A.rec_prob) {
@@ -807,7 +817,12 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
             uint32_t slot = 0;
             if (lane == 0 && mask) slot = atomicAdd(A.count_out, __popc(mask));
             slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
-            if (go) A.q_out[slot + __popc(mask & ((1u << lane) - 1u))] = path;
+            if (go) {
+                const uint32_t s = slot + __popc(mask & ((1u << lane) - 1u));
+                A.q_out[s] = path;
+                A.ray_o_out[s] = A.def_o[path];
+                A.ray_d_out[s] = A.def_d[path];
+            }
         }
         return;
     }
@@ -847,7 +862,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
         auto query = [&](bool v, uint32_t path, uint8_t* X) {
             net::Query q{mk(0.0f, 0.0f, 0.0f), mk(0.0f, 1.0f, 0.0f), mk(0.0f, 1.0f, 0.0f)};
             if (v) {
-                const float4 o4 = A.ray_o[path], d4 = A.ray_d[path], dn = A.def_n[path];
+                const float4 o4 = A.def_o[path], d4 = A.def_d[path], dn = A.def_n[path];
                 q.pos = mk(o4.x, o4.y, o4.z);
                 q.n = mk(dn.x, dn.y, dn.z);
                 q.wo = mk(-d4.x, -d4.y, -d4.z);
@@ -903,7 +918,12 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
             uint32_t slot = 0;
             if (lane == 0 && mask) slot = atomicAdd(A.count_out, __popc(mask));
             slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
-            if (go) A.q_out[slot + __popc(mask & ((1u << lane) - 1u))] = path;
+            if (go) {
+                const uint32_t s = slot + __popc(mask & ((1u << lane) - 1u));
+                A.q_out[s] = path;
+                A.ray_o_out[s] = A.def_o[path];
+                A.ray_d_out[s] = A.def_d[path];
+            }
         }
     }
     if (failed) {
@@ -1057,6 +1077,8 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
     int rc = 0;
     rc |= walloc(w, &w->ray_o, P);
     rc |= walloc(w, &w->ray_d, P);
+    rc |= walloc(w, &w->ray_o2, P);
+    rc |= walloc(w, &w->ray_d2, P);
     rc |= walloc(w, &w->hit, P);
     rc |= walloc(w, &w->queue0, P);
     rc |= walloc(w, &w->queue1, P);
@@ -1089,6 +1111,8 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
         rc |= walloc(w, &w->def_n, P);
         rc |= walloc(w, &w->def_t, P);
         rc |= walloc(w, &w->def_c, P);
+        rc |= walloc(w, &w->def_o, P);
+        rc |= walloc(w, &w->def_d, P);
         rc |= walloc(w, &w->rec_head, P);
     }
     if (rc) {
@@ -1229,7 +1253,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK) batch_generate_kernel(const __grid
         const uint32_t path = sg.path_base + j * R.npix + p;
         st = advance_fill_seed(st);
         A.seed[path] = st;
-        A.ray_o[path] = make_float4(o.x, o.y, o.z, 0.0f);
+        A.ray_o[path] = make_float4(o.x, o.y, o.z, __uint_as_float(k));
         A.ray_d[path] = make_float4(d.x, d.y, d.z, 0.0f);
         A.thr[path] = make_float4(1.0f, 1.0f, 1.0f, -1.0f);
         A.acc[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -1252,13 +1276,12 @@ __global__ void __launch_bounds__(WAVE_BLOCK) extend_batch_kernel(const __grid_c
     trace_persistent_multi<false, ALPHA>(
         n, A.work, err,
         [&](uint32_t i, float3& o, float3& d, float& t0, float& t1, const DevScene*& sp) {
-            const uint32_t path = A.q_in[i];
-            const float4 o4 = A.ray_o[path], d4 = A.ray_d[path];
+            const float4 o4 = A.ray_o[i], d4 = A.ray_d[i];
             o = make_float3(o4.x, o4.y, o4.z);
             d = make_float3(d4.x, d4.y, d4.z);
             t0 = A.tmin;
             t1 = A.tmax;
-            sp = &A.reqs[A.segs[A.flags[path] >> 16].req].S;
+            sp = &A.reqs[A.segs[__float_as_uint(o4.w)].req].S;  // the ray carries its segment
         },
         [&](uint32_t i, const TraceResult& tr) { A.hit[i] = make_uint2(tr.tri, tr.inst); });
     if (err) atomicOr(A.err, err);
@@ -1497,6 +1520,8 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         A.def_n = w->def_n;
         A.def_t = w->def_t;
         A.def_c = w->def_c;
+        A.def_o = w->def_o;
+        A.def_d = w->def_d;
         A.rec_cap = gd->opts.record_capacity;
         A.rec_count = w->ctr + 13;
         A.guide_w = gd->packed;
@@ -1536,8 +1561,11 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         uint32_t* qb = w->queue1;
         uint32_t* ca = w->ctr + 0;
         uint32_t* cb = w->ctr + 1;
+        float4 *rao = w->ray_o, *rad = w->ray_d, *rbo = w->ray_o2, *rbd = w->ray_d2;  // rays of qa, qb
         A.q_in = qa;
         A.count_in = ca;
+        A.ray_o = rao;
+        A.ray_d = rad;
         // learned guiding: record training vertices while the guide has seen fewer than train_spp
         // samples per pixel; sample the network once it has taken a training step
         const bool training = gd && gd->records && gd->trained_spp < gd->opts.train_spp;
@@ -1560,6 +1588,10 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
             A.q_out = qb;
             A.count_in = ca;
             A.count_out = cb;
+            A.ray_o = rao;
+            A.ray_d = rad;
+            A.ray_o_out = rbo;
+            A.ray_d_out = rbd;
             A.work = w->ctr + 2;
             cudaMemsetAsync(w->ctr + 2, 0, sizeof(uint32_t), st);
             cudaMemsetAsync(cb, 0, sizeof(uint32_t), st);
@@ -1593,6 +1625,8 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
             end(h);
             std::swap(qa, qb);
             std::swap(ca, cb);
+            std::swap(rao, rbo);
+            std::swap(rad, rbd);
         }
         h = begin(3);
         if (guide) {
@@ -1743,6 +1777,8 @@ static int batch_wave_buffers(BatchState* b, uint32_t capacity) {
     int rc = 0;
     rc |= walloc(w, &w->ray_o, capacity);
     rc |= walloc(w, &w->ray_d, capacity);
+    rc |= walloc(w, &w->ray_o2, capacity);
+    rc |= walloc(w, &w->ray_d2, capacity);
     rc |= walloc(w, &w->hit, capacity);
     rc |= walloc(w, &w->queue0, capacity);
     rc |= walloc(w, &w->queue1, capacity);
@@ -1891,8 +1927,11 @@ extern "C" int lam_batch_render(lam_pipeline* pl, const lam_batch_request* reqs,
             uint32_t* qb = w->queue1;
             uint32_t* ca = w->ctr + 0;
             uint32_t* cb = w->ctr + 1;
+            float4 *rao = w->ray_o, *rad = w->ray_d, *rbo = w->ray_o2, *rbd = w->ray_d2;  // rays of qa, qb
             A.q_in = qa;
             A.count_in = ca;
+            A.ray_o = rao;
+            A.ray_d = rad;
             const dim3 gp((A.pix_threads + WAVE_BLOCK - 1) / WAVE_BLOCK);
             batch_generate_kernel<<<gp, blk, 0, st>>>(A);
             for (uint32_t depth = 0; depth < pl->opts.max_depth; ++depth) {
@@ -1900,6 +1939,10 @@ extern "C" int lam_batch_render(lam_pipeline* pl, const lam_batch_request* reqs,
                 A.q_out = qb;
                 A.count_in = ca;
                 A.count_out = cb;
+                A.ray_o = rao;
+                A.ray_d = rad;
+                A.ray_o_out = rbo;
+                A.ray_d_out = rbd;
                 A.work = w->ctr + 2;
                 cudaMemsetAsync(w->ctr + 2, 0, sizeof(uint32_t), st);
                 cudaMemsetAsync(cb, 0, sizeof(uint32_t), st);
@@ -1913,6 +1956,8 @@ extern "C" int lam_batch_render(lam_pipeline* pl, const lam_batch_request* reqs,
                 launches += 2;
                 std::swap(qa, qb);
                 std::swap(ca, cb);
+                std::swap(rao, rbo);
+                std::swap(rad, rbd);
             }
             batch_accumulate_kernel<<<gp, blk, 0, st>>>(A);
             launches += 2;

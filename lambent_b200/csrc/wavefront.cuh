@@ -35,7 +35,8 @@ struct Args {
     float tmin, tmax;
     uint32_t wave_first, wave_count;
     // wave buffers
-    float4 *ray_o, *ray_d;
+    float4 *ray_o, *ray_d;          // rays by position in q_in (the generate kernel's queue is the identity)
+    float4 *ray_o_out, *ray_d_out;  // rays by position in q_out, written where a path is appended
     uint2* hit;  // (triangle slot, instance) of the closest hit, by position in the current queue
     uint32_t *q_in, *q_out;
     uint32_t *count_in, *count_out, *work;
@@ -63,6 +64,7 @@ struct Args {
     // learned guiding
     uint32_t *dq, *dq_count;
     float4 *def_n, *def_t, *def_c;
+    float4 *def_o, *def_d;  // a deferred path's origin and incoming, then outgoing, direction (by path)
     float* recs;             // training records (GUIDE_RECORD_STRIDE floats), null when not training
     uint32_t rec_cap;
     float rec_prob;          // probability that a deferred vertex is recorded
