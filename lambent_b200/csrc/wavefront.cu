@@ -408,6 +408,16 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
     for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;; base += gridDim.x * blockDim.x) {
         if (base >= n) break;
         const uint32_t i = base + lane;
+        {
+            // the next iteration's queue-ordered inputs have known addresses: start them towards L2
+            const uint32_t inext = i + gridDim.x * blockDim.x;
+            if (inext < n) {
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.q_in + inext));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.hit + inext));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.ray_o + inext));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.ray_d + inext));
+            }
+        }
         bool cont = false, deferred = false;
         uint32_t path = 0;
         v3 ro = splat(0.0f), rd = splat(0.0f);  // the outgoing ray once the bounce is shaded
