@@ -169,6 +169,8 @@ struct WaveBuffers {
     uint64_t paths = 0;
     bool full = false, guide = false;
     float4 *ray_o = nullptr, *ray_d = nullptr, *ray_o2 = nullptr, *ray_d2 = nullptr;  // two queues' rays
+    float4 *qthr0 = nullptr, *qthr1 = nullptr, *qacc0 = nullptr, *qacc1 = nullptr;  // two queues' path state
+    uint4 *qmisc0 = nullptr, *qmisc1 = nullptr;
     uint2* hit = nullptr;
     uint32_t *queue0 = nullptr, *queue1 = nullptr;
     float4 *thr = nullptr, *acc = nullptr;
@@ -261,13 +263,11 @@ __global__ void __launch_bounds__(WAVE_BLOCK) generate_kernel(Args A) {
         const uint32_t path = j * A.npix + p;
         const uint32_t fill_seed = st;
         st = advance_fill_seed(st);
-        A.seed[path] = st;
         A.ray_o[path] = make_float4(o.x, o.y, o.z, 0.0f);
         A.ray_d[path] = make_float4(d.x, d.y, d.z, 0.0f);
-        A.thr[path] = make_float4(1.0f, 1.0f, 1.0f, -1.0f);
-        A.acc[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        A.brdf[path] = 0.0f;
-        A.flags[path] = 0u;
+        A.qthr[path] = make_float4(1.0f, 1.0f, 1.0f, -1.0f);
+        A.qacc[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        A.qmisc[path] = make_uint4(0u, st, 0u, 0u);
         if (A.ort) {
             A.ort[path] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
             A.orad[path] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
@@ -422,9 +422,12 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
         uint32_t path = 0;
         v3 ro = splat(0.0f), rd = splat(0.0f);  // the outgoing ray once the bounce is shaded
         float seg_w = 0.0f;                     // a batched path's segment, carried in the ray's w
+        float4 o_thr = make_float4(0.0f, 0.0f, 0.0f, 0.0f), o_acc = o_thr;  // the outgoing state
+        uint4 o_misc = make_uint4(0u, 0u, 0u, 0u);
         if (i < n) {
             path = A.q_in[i];
-            uint32_t fl = A.flags[path];
+            const uint4 misc = A.qmisc[i];
+            uint32_t fl = misc.z;
             // per-render fields; a batched render takes them from the path's request
             const DevScene* Sp = &A.S;
             uint32_t pixel, sample_index, samples = A.samples;
@@ -451,13 +454,13 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
             ro = mk(o4.x, o4.y, o4.z);
             rd = mk(d4.x, d4.y, d4.z);
             seg_w = o4.w;
-            float4 th = A.thr[path];
+            float4 th = A.qthr[i];
             v3 color = mk(th.x, th.y, th.z);
             float picked = th.w;
-            float4 ac = A.acc[path];
+            float4 ac = A.qacc[i];
             v3 scol = mk(ac.x, ac.y, ac.z);
-            float cached_pdf = ac.w, cached_brdf = A.brdf[path];
-            uint32_t seed = A.seed[path];
+            float cached_pdf = ac.w, cached_brdf = __uint_as_float(misc.x);
+            uint32_t seed = misc.y;
             v3 orc = splat(1.0f), orad = splat(0.0f);
             float sum_mc = 0.0f;
             float4 pp = make_float4(0, 0, 0, 0), pn = make_float4(0, 0, 0, 0);
@@ -703,16 +706,20 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
             }
             if (LEARN && terminated && A.rec_head) finalize_records(A, path, scol);
             // write back
-            A.acc[path] = make_float4(scol.x, scol.y, scol.z, cached_pdf);
-            if (cont || deferred) {
-                A.thr[path] = make_float4(color.x, color.y, color.z, picked);
+            const uint32_t nfl = (fl & 0xFFFF0000u) | (depth + 1u) | (last_not_vmf ? 0x100u : 0u);
+            o_thr = make_float4(color.x, color.y, color.z, picked);
+            o_acc = make_float4(scol.x, scol.y, scol.z, cached_pdf);
+            o_misc = make_uint4(__float_as_uint(cached_brdf), seed, nfl, 0u);
+            // a finished path leaves its radiance by path for the accumulate kernel; a deferred one its
+            // whole state for the guide kernel; a continuing one goes with its queue slot (below)
+            if (!cont || deferred) A.acc[path] = o_acc;
+            if (deferred) {
+                A.thr[path] = o_thr;
                 A.brdf[path] = cached_brdf;
                 A.seed[path] = seed;
-                A.flags[path] = (fl & 0xFFFF0000u) | (depth + 1u) | (last_not_vmf ? 0x100u : 0u);
-                if (deferred) {
-                    A.def_o[path] = make_float4(ro.x, ro.y, ro.z, 0.0f);
-                    A.def_d[path] = make_float4(rd.x, rd.y, rd.z, 0.0f);
-                }
+                A.flags[path] = nfl;
+                A.def_o[path] = make_float4(ro.x, ro.y, ro.z, 0.0f);
+                A.def_d[path] = make_float4(rd.x, rd.y, rd.z, 0.0f);
             }
             if (rec) {
                 A.ort[path] = make_float4(orc.x, orc.y, orc.z, sum_mc);
@@ -738,6 +745,9 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 A.q_out[s] = path;
                 A.ray_o_out[s] = make_float4(ro.x, ro.y, ro.z, seg_w);
                 A.ray_d_out[s] = make_float4(rd.x, rd.y, rd.z, 0.0f);
+                A.qthr_out[s] = o_thr;
+                A.qacc_out[s] = o_acc;
+                A.qmisc_out[s] = o_misc;
             }
         }
         if (LEARN) {
@@ -832,6 +842,9 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
                 A.q_out[s] = path;
                 A.ray_o_out[s] = A.def_o[path];
                 A.ray_d_out[s] = A.def_d[path];
+                A.qthr_out[s] = A.thr[path];
+                A.qacc_out[s] = A.acc[path];
+                A.qmisc_out[s] = make_uint4(__float_as_uint(A.brdf[path]), A.seed[path], A.flags[path], 0u);
             }
         }
         return;
@@ -933,6 +946,9 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
                 A.q_out[s] = path;
                 A.ray_o_out[s] = A.def_o[path];
                 A.ray_d_out[s] = A.def_d[path];
+                A.qthr_out[s] = A.thr[path];
+                A.qacc_out[s] = A.acc[path];
+                A.qmisc_out[s] = make_uint4(__float_as_uint(A.brdf[path]), A.seed[path], A.flags[path], 0u);
             }
         }
     }
@@ -1089,6 +1105,12 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
     rc |= walloc(w, &w->ray_d, P);
     rc |= walloc(w, &w->ray_o2, P);
     rc |= walloc(w, &w->ray_d2, P);
+    rc |= walloc(w, &w->qthr0, P);
+    rc |= walloc(w, &w->qthr1, P);
+    rc |= walloc(w, &w->qacc0, P);
+    rc |= walloc(w, &w->qacc1, P);
+    rc |= walloc(w, &w->qmisc0, P);
+    rc |= walloc(w, &w->qmisc1, P);
     rc |= walloc(w, &w->hit, P);
     rc |= walloc(w, &w->queue0, P);
     rc |= walloc(w, &w->queue1, P);
@@ -1262,13 +1284,11 @@ __global__ void __launch_bounds__(WAVE_BLOCK) batch_generate_kernel(const __grid
     for (uint32_t j = 0; j < sg.count; ++j) {
         const uint32_t path = sg.path_base + j * R.npix + p;
         st = advance_fill_seed(st);
-        A.seed[path] = st;
         A.ray_o[path] = make_float4(o.x, o.y, o.z, __uint_as_float(k));
         A.ray_d[path] = make_float4(d.x, d.y, d.z, 0.0f);
-        A.thr[path] = make_float4(1.0f, 1.0f, 1.0f, -1.0f);
-        A.acc[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        A.brdf[path] = 0.0f;
-        A.flags[path] = k << 16;
+        A.qthr[path] = make_float4(1.0f, 1.0f, 1.0f, -1.0f);
+        A.qacc[path] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        A.qmisc[path] = make_uint4(0u, st, k << 16, 0u);
         A.q_in[path] = path;
         st = rand_u32(st);
     }
@@ -1572,10 +1592,15 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         uint32_t* ca = w->ctr + 0;
         uint32_t* cb = w->ctr + 1;
         float4 *rao = w->ray_o, *rad = w->ray_d, *rbo = w->ray_o2, *rbd = w->ray_d2;  // rays of qa, qb
+        float4 *tha = w->qthr0, *thb = w->qthr1, *aca = w->qacc0, *acb = w->qacc1;   // path state of qa, qb
+        uint4 *mia = w->qmisc0, *mib = w->qmisc1;
         A.q_in = qa;
         A.count_in = ca;
         A.ray_o = rao;
         A.ray_d = rad;
+        A.qthr = tha;
+        A.qacc = aca;
+        A.qmisc = mia;
         // learned guiding: record training vertices while the guide has seen fewer than train_spp
         // samples per pixel; sample the network once it has taken a training step
         const bool training = gd && gd->records && gd->trained_spp < gd->opts.train_spp;
@@ -1602,6 +1627,12 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
             A.ray_d = rad;
             A.ray_o_out = rbo;
             A.ray_d_out = rbd;
+            A.qthr = tha;
+            A.qacc = aca;
+            A.qmisc = mia;
+            A.qthr_out = thb;
+            A.qacc_out = acb;
+            A.qmisc_out = mib;
             A.work = w->ctr + 2;
             cudaMemsetAsync(w->ctr + 2, 0, sizeof(uint32_t), st);
             cudaMemsetAsync(cb, 0, sizeof(uint32_t), st);
@@ -1637,6 +1668,9 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
             std::swap(ca, cb);
             std::swap(rao, rbo);
             std::swap(rad, rbd);
+            std::swap(tha, thb);
+            std::swap(aca, acb);
+            std::swap(mia, mib);
         }
         h = begin(3);
         if (guide) {
@@ -1789,6 +1823,12 @@ static int batch_wave_buffers(BatchState* b, uint32_t capacity) {
     rc |= walloc(w, &w->ray_d, capacity);
     rc |= walloc(w, &w->ray_o2, capacity);
     rc |= walloc(w, &w->ray_d2, capacity);
+    rc |= walloc(w, &w->qthr0, capacity);
+    rc |= walloc(w, &w->qthr1, capacity);
+    rc |= walloc(w, &w->qacc0, capacity);
+    rc |= walloc(w, &w->qacc1, capacity);
+    rc |= walloc(w, &w->qmisc0, capacity);
+    rc |= walloc(w, &w->qmisc1, capacity);
     rc |= walloc(w, &w->hit, capacity);
     rc |= walloc(w, &w->queue0, capacity);
     rc |= walloc(w, &w->queue1, capacity);
@@ -1938,10 +1978,15 @@ extern "C" int lam_batch_render(lam_pipeline* pl, const lam_batch_request* reqs,
             uint32_t* ca = w->ctr + 0;
             uint32_t* cb = w->ctr + 1;
             float4 *rao = w->ray_o, *rad = w->ray_d, *rbo = w->ray_o2, *rbd = w->ray_d2;  // rays of qa, qb
+            float4 *tha = w->qthr0, *thb = w->qthr1, *aca = w->qacc0, *acb = w->qacc1;   // path state of qa, qb
+            uint4 *mia = w->qmisc0, *mib = w->qmisc1;
             A.q_in = qa;
             A.count_in = ca;
             A.ray_o = rao;
             A.ray_d = rad;
+            A.qthr = tha;
+            A.qacc = aca;
+            A.qmisc = mia;
             const dim3 gp((A.pix_threads + WAVE_BLOCK - 1) / WAVE_BLOCK);
             batch_generate_kernel<<<gp, blk, 0, st>>>(A);
             for (uint32_t depth = 0; depth < pl->opts.max_depth; ++depth) {
@@ -1953,6 +1998,12 @@ extern "C" int lam_batch_render(lam_pipeline* pl, const lam_batch_request* reqs,
                 A.ray_d = rad;
                 A.ray_o_out = rbo;
                 A.ray_d_out = rbd;
+                A.qthr = tha;
+                A.qacc = aca;
+                A.qmisc = mia;
+                A.qthr_out = thb;
+                A.qacc_out = acb;
+                A.qmisc_out = mib;
                 A.work = w->ctr + 2;
                 cudaMemsetAsync(w->ctr + 2, 0, sizeof(uint32_t), st);
                 cudaMemsetAsync(cb, 0, sizeof(uint32_t), st);
@@ -1968,6 +2019,9 @@ extern "C" int lam_batch_render(lam_pipeline* pl, const lam_batch_request* reqs,
                 std::swap(ca, cb);
                 std::swap(rao, rbo);
                 std::swap(rad, rbd);
+                std::swap(tha, thb);
+                std::swap(aca, acb);
+                std::swap(mia, mib);
             }
             batch_accumulate_kernel<<<gp, blk, 0, st>>>(A);
             launches += 2;

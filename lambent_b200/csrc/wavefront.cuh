@@ -37,6 +37,13 @@ struct Args {
     // wave buffers
     float4 *ray_o, *ray_d;          // rays by position in q_in (the generate kernel's queue is the identity)
     float4 *ray_o_out, *ray_d_out;  // rays by position in q_out, written where a path is appended
+    // a live path's core state by position in q_in / q_out: throughput (xyz) and picked IOR (w); radiance
+    // sum (xyz) and cached pdf (w); (cached brdf bits, seed, flags, 0).  thr / acc / brdf / seed / flags
+    // below hold the same fields by path for deferred paths, and acc the radiance of finished paths.
+    float4 *qthr, *qacc;
+    uint4* qmisc;
+    float4 *qthr_out, *qacc_out;
+    uint4* qmisc_out;
     uint2* hit;  // (triangle slot, instance) of the closest hit, by position in the current queue
     uint32_t *q_in, *q_out;
     uint32_t *count_in, *count_out, *work;
