@@ -589,7 +589,7 @@ struct Traverser {
 
 // Lanes below this many active rays trigger a refill of the idle lanes from the work queue.
 #ifndef LAM_REFILL_THRESHOLD
-#define LAM_REFILL_THRESHOLD 24
+#define LAM_REFILL_THRESHOLD 28
 #endif
 constexpr int REFILL_THRESHOLD = LAM_REFILL_THRESHOLD;
 

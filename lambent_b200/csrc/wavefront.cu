@@ -1080,8 +1080,10 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
     const uint32_t npix = width * height;
     uint32_t spp_wave = 1;
     if (!guide && pl->opts.restir_temporal != LAM_RESTIR_PER_SAMPLE) {
-        // enough paths in flight to fill the GPU: aim for ~8M paths, at most the sample count
-        uint64_t target = 8ull << 20;
+        // aim for ~32M paths in flight (about 7 GB of wave state at 1080p), at most the sample count:
+        // the deep bounces of a small wave leave the persistent traversal tail-bound (1080p, 16 spp:
+        // 1058 Mrays/s with 4-spp waves, 1089 with 8, 1104 with one 16-spp wave)
+        uint64_t target = 32ull << 20;
         spp_wave = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(pl->opts.samples, target / std::max(1u, npix)));
     }
     WaveBuffers* w = pl->wave;
@@ -1584,9 +1586,16 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         if (h >= 0) cudaEventRecord(pl->timed[h].end, st);
     };
     cudaMemsetAsync(w->ctr, 0, 10 * sizeof(uint32_t), st);  // keeps the cumulative counter ctr[10..11]
-    for (uint32_t first = 0; first < pl->opts.samples; first += w->spp_wave) {
+    for (uint32_t first = 0; first < pl->opts.samples;) {
+        // learned guiding: record training vertices while the guide has seen fewer than train_spp
+        // samples per pixel; sample the network once it has taken a training step
+        const bool training = gd && gd->records && gd->trained_spp < gd->opts.train_spp;
+        uint32_t count = std::min(w->spp_wave, pl->opts.samples - first);
+        // the guide takes steps_per_wave Adam steps after each training wave; training waves stay at
+        // ~8M paths (4 spp at 1080p) whatever the wave size of the rest of the render
+        if (training) count = std::min<uint32_t>(count, std::max<uint32_t>(1u, (uint32_t)((8ull << 20) / w->npix)));
         A.wave_first = first;
-        A.wave_count = std::min(w->spp_wave, pl->opts.samples - first);
+        A.wave_count = count;
         uint32_t* qa = w->queue0;
         uint32_t* qb = w->queue1;
         uint32_t* ca = w->ctr + 0;
@@ -1601,9 +1610,6 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         A.qthr = tha;
         A.qacc = aca;
         A.qmisc = mia;
-        // learned guiding: record training vertices while the guide has seen fewer than train_spp
-        // samples per pixel; sample the network once it has taken a training step
-        const bool training = gd && gd->records && gd->trained_spp < gd->opts.train_spp;
         const bool use_net = gd && gd->steps > 0;
         A.recs = training ? gd->records : nullptr;
         if (training) {
@@ -1693,6 +1699,7 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
             end(h);
             gd->trained_spp += A.wave_count;
         }
+        first += count;
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_error(e, "lam_render launch");

@@ -109,14 +109,26 @@ def test_statistical_agreement_independent_seeds(cuda):
     assert abs(gm.mean() - om.mean()) < 0.02 * om.mean() + 1e-3
 
 
-def test_markov_guiding_is_unbiased(cuda):
-    """Guided (Markov chains) and unguided renders converge to the same image."""
+def test_markov_guiding_matches_oracle_statistically(cuda):
+    """Markov-chain guiding on the GPU against the oracle's sequential restatement of it.
+
+    The GPU's world-grid updates race (as the reference's atomics do), so guided renders are
+    compared by their means over independent seeds, not pixel by pixel.  The restated algorithm
+    itself reads about 5 % above plain path tracing on this scene (oracle: 0.226 against 0.215 over
+    8 seeds; per-render sd 0.007), so the check against plain is a looser bound."""
     s = scenes.cornell_box(32, 32)
-    plain = np.stack([gpu_render(s, 64, restir=_abi.RESTIR_DISABLED, seed=r)["color"][..., :3] for r in range(4)]).mean(0)
+    n = 8
+    plain = np.stack([gpu_render(s, 64, restir=_abi.RESTIR_DISABLED, seed=r)["color"][..., :3] for r in range(n)])
     guided = np.stack([gpu_render(s, 64, restir=_abi.RESTIR_DISABLED, guide=_abi.GUIDE_MARKOV, seed=100 + r)["color"][..., :3]
-                       for r in range(4)]).mean(0)
+                       for r in range(n)])
     assert np.isfinite(guided).all()
-    assert abs(guided.mean() - plain.mean()) < 0.08 * plain.mean()
+    osc = O.OracleScene(s)
+    o_guided = np.stack([osc.render(s.camera, 32, 32, samples=64, restir=_abi.RESTIR_DISABLED, guide=_abi.GUIDE_MARKOV,
+                                    seed_offset=100 + r)["color"][..., :3] for r in range(n)])
+    pm, gm, om = plain.mean(), guided.mean(), o_guided.mean()
+    # means of 8 renders: standard error ~0.0025 each, so 0.06 of the mean is about 4 standard errors
+    assert abs(gm - om) < 0.06 * pm, (gm, om, pm)
+    assert abs(gm - pm) < 0.12 * pm, (gm, pm)
 
 
 def test_depth_and_layout_errors(cuda):
