@@ -455,6 +455,13 @@ int lam_render_stats_get(const lam_pipeline* pipeline, lam_render_stats* out);
  * CUDA events around its launches; lam_render_profile_get synchronises and sums them. */
 int lam_pipeline_set_profiling(lam_pipeline* pipeline, int enabled);
 int lam_render_profile_get(lam_pipeline* pipeline, lam_stage_times* out);
+/* Wave size (no counterpart in the reference, whose rt_main holds one pixel's samples in a thread):
+ * lam_render runs a frame's samples in waves of at most max(pixels, max_paths) paths; each path in
+ * flight keeps about 220 bytes of device state.  0 restores the default of about 32M paths (one
+ * 16-spp wave at 1080p, about 7 GB).  Markov guiding and per-sample ReSTIR always run one sample per
+ * wave.  The image does not depend on the wave size; smaller waves trade speed for memory.  Takes
+ * effect at the next lam_render. */
+int lam_pipeline_set_wave_paths(lam_pipeline* pipeline, uint64_t max_paths);
 int lam_render_profile_reset(lam_pipeline* pipeline);
 
 /* TemporalResampling main, src/importance_sampling/temporal_resampling.wesl:37-65 */

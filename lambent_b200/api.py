@@ -85,6 +85,7 @@ def lib():
     _sig(L, "lam_render", i, vp, vp, vp, P(_CCamera), P(FrameTargets), u32, vp)
     _sig(L, "lam_render_stats_get", i, vp, P(RenderStats))
     _sig(L, "lam_pipeline_set_profiling", i, vp, i)
+    _sig(L, "lam_pipeline_set_wave_paths", i, vp, C.c_uint64)
     _sig(L, "lam_render_profile_get", i, vp, P(_abi.StageTimes))
     _sig(L, "lam_render_profile_reset", i, vp)
     _sig(L, "lam_temporal_resampling", i, vp, u32, u32, u32, vp)
@@ -416,6 +417,10 @@ class Pipeline:
 
     def set_profiling(self, enabled=True):
         check(lib().lam_pipeline_set_profiling(self._h, 1 if enabled else 0))
+
+    def set_wave_paths(self, max_paths=0):
+        """Bounds the paths of one wave (device memory ~220 B per path); 0 restores the default."""
+        check(lib().lam_pipeline_set_wave_paths(self._h, int(max_paths)))
 
     def profile(self):
         t = _abi.StageTimes()

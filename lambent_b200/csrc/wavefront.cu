@@ -1083,7 +1083,7 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
         // aim for ~32M paths in flight (about 7 GB of wave state at 1080p), at most the sample count:
         // the deep bounces of a small wave leave the persistent traversal tail-bound (1080p, 16 spp:
         // 1058 Mrays/s with 4-spp waves, 1089 with 8, 1104 with one 16-spp wave)
-        uint64_t target = 32ull << 20;
+        uint64_t target = pl->wave_paths ? pl->wave_paths : (32ull << 20);
         spp_wave = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(pl->opts.samples, target / std::max(1u, npix)));
     }
     WaveBuffers* w = pl->wave;
@@ -1384,6 +1384,12 @@ extern "C" int lam_pipeline_destroy(lam_pipeline* p) {
     }
     for (cudaEvent_t e : p->event_pool) cudaEventDestroy(e);
     delete p;
+    return LAM_OK;
+}
+
+extern "C" int lam_pipeline_set_wave_paths(lam_pipeline* p, uint64_t max_paths) {
+    if (!p) return set_error(LAM_ERR_INVALID_ARGUMENT, "null pipeline");
+    p->wave_paths = max_paths;
     return LAM_OK;
 }
 
