@@ -31,7 +31,12 @@ SEG_BYTES_TOTAL = 280   # extend 48 + shade 232 (compulsory wavefront traffic pe
 # DRAM bytes (read + write) per segment of the extend kernel, from one ncu capture of all extend
 # launches of a 960x540, 4-spp render of the same scene (profiles/extend_kernel_icosphere_field_960x540.md);
 # traffic grows with the segments processed, so a full launch's traffic is this times its segments.
-EXTEND_DRAM_BYTES_PER_SEGMENT = 188.0
+EXTEND_DRAM_BYTES_PER_SEGMENT = 138.0
+# What does bound the traversal kernel, from the same kind of capture (ncu --set full of two extend
+# launches of the 960x540 case; profiles/extend_kernel_icosphere_field_960x540.md): instruction issue.
+EXTEND_MEASURED_BOUND = {"kind": "instruction issue (BVH and triangles stay in L2)", "issue_slots_busy": 0.727,
+                         "alu_pipe": 0.562, "fma_pipe": 0.250, "dram_throughput": 0.012, "l2_hit_rate": 0.850,
+                         "threads_per_instruction": 18.3}
 
 
 def parse():
@@ -558,7 +563,8 @@ def run_ours(a):
                                          "run's segments per launch (BVH and triangle fetches that miss L2)",
                          "extend_ms": round(prof.extend_ms, 3), "shade_ms": round(prof.shade_ms, 3),
                          "generate_ms": round(prof.generate_ms, 3), "accumulate_ms": round(prof.accumulate_ms, 3),
-                         "shade_gbs": round(shade_gbs, 2)},
+                         "shade_gbs": round(shade_gbs, 2),
+                         "measured_bound": EXTEND_MEASURED_BOUND},
             "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 128,
                     "d2h_bytes_per_step": H * W * 16},
             "gpu_launches": int(launches),
