@@ -36,7 +36,8 @@ EXTEND_DRAM_BYTES_PER_SEGMENT = 138.0
 # launches of the 960x540 case; profiles/extend_kernel_icosphere_field_960x540.md): instruction issue.
 EXTEND_MEASURED_BOUND = {"kind": "instruction issue (BVH and triangles stay in L2)", "issue_slots_busy": 0.727,
                          "alu_pipe": 0.562, "fma_pipe": 0.250, "dram_throughput": 0.012, "l2_hit_rate": 0.850,
-                         "threads_per_instruction": 18.3}
+                         "threads_per_instruction": 18.3, "l2_gbs": 3290.0,
+                         "l2_note": "lts__t_sectors x 32 B / duration of the captured launch (node and triangle reads)"}
 
 
 def parse():
@@ -564,7 +565,12 @@ def run_ours(a):
                          "extend_ms": round(prof.extend_ms, 3), "shade_ms": round(prof.shade_ms, 3),
                          "generate_ms": round(prof.generate_ms, 3), "accumulate_ms": round(prof.accumulate_ms, 3),
                          "shade_gbs": round(shade_gbs, 2),
-                         "measured_bound": EXTEND_MEASURED_BOUND},
+                         "measured_bound": EXTEND_MEASURED_BOUND,
+                         # the whole wavefront against HBM: compulsory bytes per segment (extend 48 +
+                         # shade 232) at the achieved segment rate
+                         "pipeline": {"bytes_per_segment": SEG_BYTES_TOTAL,
+                                      "achieved": round(value * 1e6 * SEG_BYTES_TOTAL / 1e9, 2),
+                                      "frac": round(value * 1e6 * SEG_BYTES_TOTAL / 1e9 / hbm, 5)}},
             "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 128,
                     "d2h_bytes_per_step": H * W * 16},
             "gpu_launches": int(launches),
