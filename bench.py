@@ -566,11 +566,11 @@ def run_ours(a):
                          "generate_ms": round(prof.generate_ms, 3), "accumulate_ms": round(prof.accumulate_ms, 3),
                          "shade_gbs": round(shade_gbs, 2),
                          "measured_bound": EXTEND_MEASURED_BOUND,
-                         # the whole wavefront against HBM: compulsory bytes per segment (extend 48 +
-                         # shade 232) at the achieved segment rate
+                         # the whole wavefront against one GPU's HBM: compulsory bytes per segment
+                         # (extend 48 + shade 232) at the achieved segment rate per GPU
                          "pipeline": {"bytes_per_segment": SEG_BYTES_TOTAL,
-                                      "achieved": round(value * 1e6 * SEG_BYTES_TOTAL / 1e9, 2),
-                                      "frac": round(value * 1e6 * SEG_BYTES_TOTAL / 1e9 / hbm, 5)}},
+                                      "achieved": round(value / world * 1e6 * SEG_BYTES_TOTAL / 1e9, 2),
+                                      "frac": round(value / world * 1e6 * SEG_BYTES_TOTAL / 1e9 / hbm, 5)}},
             "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 128,
                     "d2h_bytes_per_step": H * W * 16},
             "gpu_launches": int(launches),
