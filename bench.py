@@ -66,6 +66,9 @@ def parse():
     p.add_argument("--guided-train-spp", type=int, default=32)
     p.add_argument("--guided-steps-per-wave", type=int, default=25)
     p.add_argument("--no-batched", action="store_true", help="skip the batched-serving measurement")
+    p.add_argument("--no-restir", action="store_true", help="skip the ReSTIR GI frame-loop measurement")
+    p.add_argument("--restir-only", action="store_true", help="run only the ReSTIR GI frame-loop measurement")
+    p.add_argument("--restir-frames", type=int, default=120)
     p.add_argument("--batched-only", action="store_true", help="run only the batched-serving measurement")
     p.add_argument("--batched-requests", type=int, default=64)
     p.add_argument("--batched-scenes", type=int, default=8, help="distinct scenes shared by the requests")
@@ -346,6 +349,79 @@ def guided_equal_time(a, dev):
     }
 
 
+def restir_frames(a, dev):
+    """ReSTIR GI frame loop: the Cornell box at 1920x1080, a 120-frame camera orbit at 1 spp per frame,
+    per-pixel reservoirs, Markov-chain guiding, then temporal resampling, spatial resampling (5
+    samples in a 61-pixel window) and the end-of-frame advance with M capped at 20, as the reference
+    example drives them.  CUDA events around each pass give the split; 5 untimed frames first."""
+    import math
+    import torch
+    import lambent_b200 as lb
+    from lambent_b200 import _abi, scenes
+    W, H = 1920, 1080
+    s = scenes.cornell_box(W, H)
+    gs = lb.GpuScene(s)
+    world = 1_500_000
+    bufs = lb.DataBuffers(W, H, world, _abi.BUFFER_ALL)
+    pipe = lb.RayTracer(lb.path_tracing.Medium).create_pipeline(*s.layout_counts(), lb.PathTracerOpts(
+        samples=1, restir_temporal=_abi.RESTIR_PER_PIXEL, max_depth=8, guide_mode=_abi.GUIDE_MARKOV))
+    col = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
+    tg = lb.targets_from(col)
+    stream = torch.cuda.current_stream()
+    cams = []
+    for f in range(a.restir_frames):
+        th = math.radians(12.0) * math.sin(2.0 * math.pi * f / a.restir_frames)
+        cams.append(scenes.make_camera((3.4 * math.sin(th), 1.0, 3.4 * math.cos(th)), (0.0, 1.0, 0.0), 40.0, W / H))
+    adv = lb.AdvanceOptions(20)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    split = [0.0, 0.0, 0.0, 0.0]
+
+    def frame(f, timed):
+        if timed:
+            ev[0].record(stream)
+        pipe.render(gs, bufs, cams[f % len(cams)], tg, f, stream)
+        if timed:
+            ev[1].record(stream)
+        bufs.temporal_resampling(f, stream)
+        if timed:
+            ev[2].record(stream)
+        bufs.spatial_resampling(tg, 5, 61, f, stream)
+        if timed:
+            ev[3].record(stream)
+        bufs.advance_frame(_abi.BUFFER_ALL, adv, stream)
+        if timed:
+            ev[4].record(stream)
+            torch.cuda.synchronize()
+            for k in range(4):
+                split[k] += ev[k].elapsed_time(ev[k + 1])
+
+    for f in range(5):
+        frame(f, False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for f in range(a.restir_frames):
+        frame(f, False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    pipe.set_profiling(True)  # segment count of the split frames
+    pipe.profile_reset()
+    for f in range(8):  # the split, from separately timed frames (events synchronise each frame)
+        frame(f, True)
+    segs_per_frame = pipe.profile().ray_segments / 8
+    pipe.set_profiling(False)
+    assert pipe.stats().error_flags == 0, "ReSTIR frame loop reported an error"
+    n = a.restir_frames
+    return {"config": {"workload": f"Cornell box (36 tris), {W}x{H}, {n}-frame orbit, 1 spp/frame, depth 8, "
+                                   "Medium, per-pixel reservoirs, Markov chains (1.5M world cells), temporal + "
+                                   "spatial (5 samples, 61-px window), M cap 20"},
+            "frames": n, "ms_per_frame": round(ms / n, 3), "frames_per_s": round(n / (ms / 1e3), 2),
+            "render_mrays_per_s": round(segs_per_frame / (split[0] / 8 / 1e3) / 1e6, 1),
+            "split_ms_per_frame": {"render": round(split[0] / 8, 3), "temporal": round(split[1] / 8, 3),
+                                   "spatial": round(split[2] / 8, 3), "advance": round(split[3] / 8, 3)}}
+
+
 def batched_serving(a, dev):
     """Batched serving-style render: independent requests in one lam_batch_render, replayed as a
     CUDA graph with the autotuner's queue and launch sizes.
@@ -581,13 +657,15 @@ def run_ours(a):
         }
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_reference(a, scene, a.cpu_seconds)
-        if world == 1 and not (a.no_guided and a.no_batched):
+        if world == 1 and not (a.no_guided and a.no_batched and a.no_restir):
             del gscene, pipe, bufs
             torch.cuda.empty_cache()
         if not a.no_guided and world == 1:
             line["guided"] = guided_equal_time(a, dev)
         if not a.no_batched and world == 1:
             line["batched"] = batched_serving(a, dev)
+        if not a.no_restir and world == 1:
+            line["restir"] = restir_frames(a, dev)
         emit(line, a)
     if world > 1:
         dist.destroy_process_group()
@@ -601,6 +679,10 @@ def main():
         import torch
         torch.cuda.set_device(0)
         emit({"metric": "batched serving samples/s", "batched": batched_serving(a, torch.device("cuda", 0))}, a)
+    elif a.restir_only:
+        import torch
+        torch.cuda.set_device(0)
+        emit({"metric": "ReSTIR GI frame loop", "restir": restir_frames(a, torch.device("cuda", 0))}, a)
     elif a.guided_only:
         import torch
         torch.cuda.set_device(0)
