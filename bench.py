@@ -185,7 +185,7 @@ def run_reference(a):
     from lambent_b200 import _abi
     osc = O.OracleScene(scene)
     cores = os.cpu_count() or 1
-    side = 256  # large enough that the host threads' start-up does not dominate a step
+    side = min(256, a.width, a.height)  # large enough that the host threads' start-up does not dominate a step
     segs = 0
     tot = 0.0
     for k in range(a.warmup + a.steps):
