@@ -460,7 +460,9 @@ int lam_render_profile_get(lam_pipeline* pipeline, lam_stage_times* out);
  * flight keeps about 220 bytes of device state.  0 restores the default of about 32M paths (one
  * 16-spp wave at 1080p, about 7 GB).  Markov guiding and per-sample ReSTIR always run one sample per
  * wave.  The image does not depend on the wave size; smaller waves trade speed for memory.  Takes
- * effect at the next lam_render. */
+ * effect at the next lam_render.  lam_render itself caps a new wave at half the free device memory
+ * and halves it while an allocation fails; a wave shrunk that way is kept for later, larger
+ * requests. */
 int lam_pipeline_set_wave_paths(lam_pipeline* pipeline, uint64_t max_paths);
 int lam_render_profile_reset(lam_pipeline* pipeline);
 

@@ -168,6 +168,7 @@ struct WaveBuffers {
     uint32_t width = 0, height = 0, npix = 0, spp_wave = 0;
     uint64_t paths = 0;
     bool full = false, guide = false;
+    bool mem_capped = false;  // spp_wave was reduced to fit device memory
     float4 *ray_o = nullptr, *ray_d = nullptr, *ray_o2 = nullptr, *ray_d2 = nullptr;  // two queues' rays
     float4 *qthr0 = nullptr, *qthr1 = nullptr, *qacc0 = nullptr, *qacc1 = nullptr;  // two queues' path state
     uint4 *qmisc0 = nullptr, *qmisc1 = nullptr;
@@ -1076,31 +1077,11 @@ __global__ void shuffle_kernel(Args A) {
     mc_store(A.tent_snap + p, t);
 }
 
-static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool full, bool guide, bool learned) {
-    const uint32_t npix = width * height;
-    uint32_t spp_wave = 1;
-    if (!guide && pl->opts.restir_temporal != LAM_RESTIR_PER_SAMPLE) {
-        // aim for ~32M paths in flight (about 7 GB of wave state at 1080p), at most the sample count:
-        // the deep bounces of a small wave leave the persistent traversal tail-bound (1080p, 16 spp:
-        // 1058 Mrays/s with 4-spp waves, 1089 with 8, 1104 with one 16-spp wave)
-        uint64_t target = pl->wave_paths ? pl->wave_paths : (32ull << 20);
-        spp_wave = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(pl->opts.samples, target / std::max(1u, npix)));
-    }
-    WaveBuffers* w = pl->wave;
-    if (w && w->width == width && w->height == height && w->spp_wave == spp_wave && w->full == full && w->guide == guide &&
-        w->learned == learned)
-        return LAM_OK;
-    free_wave(w);
-    pl->wave = nullptr;
-    w = new WaveBuffers();
-    w->width = width;
-    w->height = height;
-    w->npix = npix;
-    w->spp_wave = spp_wave;
-    w->paths = (uint64_t)npix * spp_wave;
-    w->full = full;
-    w->guide = guide;
-    w->learned = learned;
+// Device bytes of wave state per path: rays of two queues (64), live state of two queues (96), hit
+// (8), two queue entries (8), state by path (44); ReSTIR / Markov / learned-guide extras.
+constexpr uint64_t WAVE_BYTES_PER_PATH = 220, WAVE_BYTES_FULL = 96, WAVE_BYTES_GUIDE = 32, WAVE_BYTES_LEARNED = 88;
+
+static int alloc_wave(WaveBuffers* w, uint32_t npix, bool full, bool guide, bool learned) {
     const size_t P = w->paths;
     int rc = 0;
     rc |= walloc(w, &w->ray_o, P);
@@ -1149,10 +1130,56 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
         rc |= walloc(w, &w->def_d, P);
         rc |= walloc(w, &w->rec_head, P);
     }
-    if (rc) {
-        free_wave(w);
-        return LAM_ERR_CUDA;
+    return rc;
+}
+
+static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool full, bool guide, bool learned) {
+    const uint32_t npix = width * height;
+    uint32_t spp_wave = 1;
+    if (!guide && pl->opts.restir_temporal != LAM_RESTIR_PER_SAMPLE) {
+        // aim for ~32M paths in flight (about 7 GB of wave state at 1080p), at most the sample count:
+        // the deep bounces of a small wave leave the persistent traversal tail-bound (1080p, 16 spp:
+        // 1058 Mrays/s with 4-spp waves, 1089 with 8, 1104 with one 16-spp wave)
+        uint64_t target = pl->wave_paths ? pl->wave_paths : (32ull << 20);
+        spp_wave = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(pl->opts.samples, target / std::max(1u, npix)));
     }
+    WaveBuffers* w = pl->wave;
+    // a wave that was shrunk to fit device memory is kept while the request is larger
+    if (w && w->width == width && w->height == height && w->full == full && w->guide == guide && w->learned == learned &&
+        (w->spp_wave == spp_wave || (w->mem_capped && w->spp_wave < spp_wave)))
+        return LAM_OK;
+    free_wave(w);
+    pl->wave = nullptr;
+    // at most half of the free device memory; if an allocation still fails, halve the wave
+    bool capped = false;
+    size_t free_b = 0, total_b = 0;
+    if (spp_wave > 1 && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        const uint64_t per_path = WAVE_BYTES_PER_PATH + (full ? WAVE_BYTES_FULL : 0) + (guide ? WAVE_BYTES_GUIDE : 0) +
+                                  (learned ? WAVE_BYTES_LEARNED : 0);
+        const uint64_t fit = (uint64_t)(free_b / 2) / (per_path * std::max(1u, npix));
+        if (fit < spp_wave) {
+            spp_wave = (uint32_t)std::max<uint64_t>(1, fit);
+            capped = true;
+        }
+    }
+    for (;;) {
+        w = new WaveBuffers();
+        w->width = width;
+        w->height = height;
+        w->npix = npix;
+        w->spp_wave = spp_wave;
+        w->paths = (uint64_t)npix * spp_wave;
+        w->full = full;
+        w->guide = guide;
+        w->learned = learned;
+        if (alloc_wave(w, npix, full, guide, learned) == LAM_OK) break;
+        free_wave(w);
+        if (spp_wave == 1) return LAM_ERR_CUDA;  // the failed allocation set the error message
+        (void)cudaGetLastError();                // an out-of-memory error is not sticky
+        spp_wave = std::max(1u, spp_wave / 2u);
+        capped = true;
+    }
+    w->mem_capped = capped;
     cudaMemset(w->ctr, 0, 64 * sizeof(uint32_t));
     pl->total_segments = 0;
     pl->prof_segments_base = 0;
