@@ -2139,7 +2139,7 @@ extern "C" int lam_batch_autotune(lam_pipeline* pl, const lam_batch_request* req
     float best_ms = 3.0e38f;
     int rc = LAM_OK;
     // coordinate 1: queue size
-    for (uint32_t wp : {2u << 20, 4u << 20, 8u << 20, 16u << 20}) {
+    for (uint32_t wp : {2u << 20, 4u << 20, 8u << 20, 16u << 20, 32u << 20}) {
         lam_batch_tuning t = best;
         t.wave_paths = wp;
         float ms = 0;
