@@ -587,11 +587,18 @@ def run_ours(a):
         ms_max, segs_total = ms, float(segs)
     value = segs_total / (ms_max / 1e3) / 1e6
 
-    # e2e through the public API with host buffers: camera H2D + render + colour D2H per step
+    # e2e through the public API with host buffers: camera H2D + render + colour D2H per step.  Two
+    # target sets: frame k's readback (on a copy stream) overlaps frame k+1's render, and a target is
+    # rendered into again only after its previous readback has finished.
     pinned_cam = torch.empty(32, dtype=torch.float32).pin_memory()
     pinned_cam.copy_(torch.tensor(list(scene.camera.c.projection_inverse) + list(scene.camera.c.view_inverse)))
     cam_dev = torch.empty(32, dtype=torch.float32, device=dev)
-    host_img = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    colors = [color, torch.zeros_like(color)]
+    tgs = [tg, lb.targets_from(colors[1], torch.zeros_like(color), torch.zeros_like(color))]
+    host_imgs = [torch.empty((H, W, 4), dtype=torch.float32).pin_memory() for _ in range(2)]
+    copy_stream = torch.cuda.Stream(device=dev)
+    rendered = [torch.cuda.Event() for _ in range(2)]
+    copied = [torch.cuda.Event() for _ in range(2)]
     pipe.profile_reset()
     pipe.set_profiling(True)
     barrier()
@@ -599,9 +606,18 @@ def run_ours(a):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for k in range(a.steps):
+        b = k % 2
+        if k >= 2:
+            stream.wait_event(copied[b])
         cam_dev.copy_(pinned_cam, non_blocking=True)
-        pipe.render(gscene, bufs, scene.camera, tg, seed0 + 7777 + k, stream)
-        host_img.copy_(color, non_blocking=True)
+        pipe.render(gscene, bufs, scene.camera, tgs[b], seed0 + 7777 + k, stream)
+        rendered[b].record(stream)
+        copy_stream.wait_event(rendered[b])
+        with torch.cuda.stream(copy_stream):
+            host_imgs[b].copy_(colors[b], non_blocking=True)
+        copied[b].record(copy_stream)
+    for b in range(min(2, a.steps)):
+        stream.wait_event(copied[b])
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
