@@ -200,6 +200,69 @@ LAM_DEV void grid_add_radiance(const Grid& g, v3 pos, v3 normal, v3 incoming, v3
     vstore(e + W_TIMEOUT, CACHE_TIMEOUT);
 }
 
+// Warp-aggregated forms of grid_add_radiance and grid_store, for lanes of a warp that call them
+// together.  Lanes whose updates address the same cell (primary index and secondary tag) act as
+// one group.  For radiance, the group claims the cell and takes its try-lock once, and the leader
+// applies every member's sample in lane order; for a chain store, the group's last lane writes.
+// Either is the state that the members' own updates leave when they run one after another without
+// contention, an outcome the reference's relaxed atomics allow (general.wesl:228-311).  Adjacent
+// pixels, which share cells at the first bounces, then no longer queue on one lock and one line.
+LAM_DEV void grid_add_radiance_warp(const Grid& g, v3 pos, v3 normal, v3 incoming, v3 radiance) {
+    const IVec l = grid_loc(g, pos);
+    const uint64_t idx = primary_hash(l, normal, incoming) % g.len;
+    const uint32_t sec = secondary_hash(l, normal);
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned grp = __match_any_sync(__activemask(), (idx << 32) | sec);
+    const uint32_t leader = __ffs(grp) - 1u;
+    uint32_t* e = g.world + idx * W_STRIDE;
+    const v3 c = clamp3(radiance, 0.0f, 100.0f);
+    int ok = 0;
+    float lum[3] = {0.0f, 0.0f, 0.0f};
+    uint32_t num = 0u;
+    if (lane == leader) {
+        ok = 1;
+        if (vload(e + W_SEC) != sec && atomicCAS(e + W_SEC, 0u, sec) != 0u) ok = 0;
+        // try-lock: a locked cell is skipped (the shader must make forward progress)
+        if (ok && atomicExch(e + W_LOCK, 1u) == 1u) ok = 0;
+        if (ok) {
+            __threadfence();
+            num = vload(e + W_NUM);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) lum[k] = __uint_as_float(vload(e + W_LUM + k));
+        }
+    }
+    if (!__shfl_sync(grp, ok, leader)) return;
+    uint32_t added = 0u;
+    for (unsigned m = grp; m; m &= m - 1u) {
+        const uint32_t src = __ffs(m) - 1u;
+        const float cx = __shfl_sync(grp, c.x, src), cy = __shfl_sync(grp, c.y, src), cz = __shfl_sync(grp, c.z, src);
+        if (lane == leader && num + added < MAX_NUM_SAMPLES) {
+            ++added;
+            lum[0] = fmaxf(strip_nan(cx + lum[0]), 0.0f);
+            lum[1] = fmaxf(strip_nan(cy + lum[1]), 0.0f);
+            lum[2] = fmaxf(strip_nan(cz + lum[2]), 0.0f);
+        }
+    }
+    if (lane == leader) {
+        if (added) {
+            atomicAdd(e + W_NUM, added);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) vstore(e + W_LUM + k, __float_as_uint(lum[k]));
+        }
+        __threadfence();
+        atomicExch(e + W_LOCK, 0u);
+        vstore(e + W_TIMEOUT, CACHE_TIMEOUT);
+    }
+}
+
+LAM_DEV void grid_store_warp(const Grid& g, v3 pos, v3 normal, v3 incoming, const MC& st) {
+    const IVec l = grid_loc(g, pos);
+    const uint64_t idx = primary_hash(l, normal, incoming) % g.len;
+    const uint32_t sec = secondary_hash(l, normal);
+    const unsigned grp = __match_any_sync(__activemask(), (idx << 32) | sec);
+    if ((threadIdx.x & 31u) == 31u - __clz(grp)) grid_store(g, pos, normal, incoming, st);
+}
+
 LAM_DEV v3 light_dir(const MC& s, v3 cur) { return safe_div3(s.light, s.weight_sum) - cur; }
 
 LAM_DEV float get_kappa(const MC& s) {

@@ -491,13 +491,13 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                     v3 est = GUIDE ? grid_radiance(G, new_pos, is.normal, rd) : splat(0.0f);
                     v3 rad_refl = strip_nan3(((is.color * est) * cached_brdf) / cached_pdf);
                     v3 rad_out = (is.emission * cached_brdf) / cached_pdf;
-                    if (GUIDE) grid_add_radiance(G, ro, last_normal, last_dir, rad_out + rad_refl);
+                    if (GUIDE) grid_add_radiance_warp(G, ro, last_normal, last_dir, rad_out + rad_refl);
                     float weight = len(rad_out + rad_refl);
                     if (weight > 0.0f) {
                         if (GUIDE) {
                             MC st = update_chain(ro, new_pos, weight, seed, false, grid_load(G, ro, last_normal, last_dir, false),
                                                  1.0f, sum_mc);
-                            grid_store(G, ro, last_normal, last_dir, st);
+                            grid_store_warp(G, ro, last_normal, last_dir, st);
                             tentative = update_chain(ro, new_pos, len(rad_out), seed, last_not_vmf, tentative,
                                                      depth == 1u ? 1.0f : 0.5f, sum_mc);
                         }
@@ -675,13 +675,13 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 if (depth != 0u) {
                     orad = fma3(orc, bg, orad);
                     v3 rad_out = (bg * cached_brdf) / cached_pdf;
-                    if (GUIDE) grid_add_radiance(G, ro, last_normal, last_dir, rad_out);
+                    if (GUIDE) grid_add_radiance_warp(G, ro, last_normal, last_dir, rad_out);
                     float weight = len(rad_out);
                     if (weight > 0.0f) {
                         if (GUIDE) {
                             MC st = update_chain(ro, new_pos, weight, seed, false, grid_load(G, ro, last_normal, last_dir, false),
                                                  1.0f, sum_mc);
-                            grid_store(G, ro, last_normal, last_dir, st);
+                            grid_store_warp(G, ro, last_normal, last_dir, st);
                             tentative = update_chain(ro, new_pos, len(rad_out), seed, false, tentative,
                                                      depth == 1u ? 1.0f : 0.5f, sum_mc);
                         }
@@ -702,8 +702,8 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 }
                 MC wc = grid_load(G, spt, snm, start_dir, false);
                 MC st = update_chain(spt, mk(vp.x, vp.y, vp.z), len(orad), seed, false, wc, 1.0f, sum_mc);
-                grid_store(G, spt, snm, start_dir, st);
-                grid_add_radiance(G, spt, snm, start_dir, orad);
+                grid_store_warp(G, spt, snm, start_dir, st);
+                grid_add_radiance_warp(G, spt, snm, start_dir, orad);
             }
             if (LEARN && terminated && A.rec_head) finalize_records(A, path, scol);
             // write back
