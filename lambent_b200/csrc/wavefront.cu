@@ -55,8 +55,12 @@ LAM_DEV void make_isect(const DevScene& S, const DevInstance* insts, uint2 hit, 
         tg = mk(pb.x, pb.y, pb.z);
     } else {
         float m[12];
-#pragma unroll
-        for (int q = 0; q < 12; ++q) m[q] = insts[hit.y].inv[q];
+        {
+            const float4* ip = reinterpret_cast<const float4*>(insts + hit.y);
+            const float4 a0 = __ldg(ip), a1 = __ldg(ip + 1), a2 = __ldg(ip + 2);
+            m[0] = a0.x; m[1] = a0.y; m[2] = a0.z; m[3] = a0.w; m[4] = a1.x; m[5] = a1.y;
+            m[6] = a1.z; m[7] = a1.w; m[8] = a2.x; m[9] = a2.y; m[10] = a2.z; m[11] = a2.w;
+        }
         float3 oo, od;
         object_ray(m, o, d, &oo, &od);
         const float4 b = __ldg(tp + 1), c = __ldg(tp + 2);
@@ -306,7 +310,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK) extend_kernel(Args A) {
     trace_persistent<false, ALPHA>(
         A.S, tl, in, n, A.work, err,
         [&](uint32_t i, float3& o, float3& d, float& t0, float& t1) {
-            const float4 o4 = A.ray_o[i], d4 = A.ray_d[i];
+            const float4 o4 = __ldg(A.ray_o + i), d4 = __ldg(A.ray_d + i);
             o = make_float3(o4.x, o4.y, o4.z);
             d = make_float3(d4.x, d4.y, d4.z);
             t0 = A.tmin;
@@ -427,7 +431,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
         uint4 o_misc = make_uint4(0u, 0u, 0u, 0u);
         if (i < n) {
             path = A.q_in[i];
-            const uint4 misc = A.qmisc[i];
+            const uint4 misc = __ldg(A.qmisc + i);
             uint32_t fl = misc.z;
             // per-render fields; a batched render takes them from the path's request
             const DevScene* Sp = &A.S;
@@ -451,14 +455,14 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
             const bool last_sample = sample_index + 1u == samples;
             const uint32_t depth = fl & 0xFFu;
             bool last_not_vmf = (fl >> 8) & 1u;
-            const float4 o4 = A.ray_o[i], d4 = A.ray_d[i];
+            const float4 o4 = __ldg(A.ray_o + i), d4 = __ldg(A.ray_d + i);
             ro = mk(o4.x, o4.y, o4.z);
             rd = mk(d4.x, d4.y, d4.z);
             seg_w = o4.w;
-            float4 th = A.qthr[i];
+            float4 th = __ldg(A.qthr + i);
             v3 color = mk(th.x, th.y, th.z);
             float picked = th.w;
-            float4 ac = A.qacc[i];
+            float4 ac = __ldg(A.qacc + i);
             v3 scol = mk(ac.x, ac.y, ac.z);
             float cached_pdf = ac.w, cached_brdf = __uint_as_float(misc.x);
             uint32_t seed = misc.y;
@@ -480,7 +484,11 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 last_dir = mk(b.x, b.y, b.z);
             }
             MC tentative = GUIDE ? mc_load(A.tent_live + pixel) : mc_zero();
-            const uint2 h = A.hit[i];  // hits are stored by queue position (extend shares this queue)
+#ifdef LAM_LDG2
+            const uint2 h = __ldg(A.hit + i);
+#else
+            const uint2 h = A.hit[i];
+#endif  // hits are stored by queue position (extend shares this queue)
             bool terminated = false;
             if (h.x != NO_HIT) {
                 Isect is;
