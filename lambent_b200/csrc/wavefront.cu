@@ -484,11 +484,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 last_dir = mk(b.x, b.y, b.z);
             }
             MC tentative = GUIDE ? mc_load(A.tent_live + pixel) : mc_zero();
-#ifdef LAM_LDG2
-            const uint2 h = __ldg(A.hit + i);
-#else
-            const uint2 h = A.hit[i];
-#endif  // hits are stored by queue position (extend shares this queue)
+            const uint2 h = __ldg(A.hit + i);  // hits are stored by queue position (extend shares this queue)
             bool terminated = false;
             if (h.x != NO_HIT) {
                 Isect is;
