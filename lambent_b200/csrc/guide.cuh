@@ -99,12 +99,22 @@ LAM_DEV uint32_t secondary_hash(IVec l, v3 normal) {
     return (rand_u32(h) ^ (n * 155096983u)) | 1u;
 }
 
+// Two adjacent words in one volatile access.  Grid cells are 56 bytes in cudaMalloc'd buffers and
+// every pair starts at an even word, so the access is 8-byte aligned.  Reading two fields at once is
+// one of the interleavings the reference's separate relaxed atomic loads allow.
+LAM_DEV uint2 vload2(const uint32_t* p) {
+    uint2 v;
+    asm volatile("ld.volatile.global.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+    return v;
+}
+
 LAM_DEV MC read_chain(const uint32_t* e) {
     MC s;
-    s.light = mk(__uint_as_float(vload(e + W_CL)), __uint_as_float(vload(e + W_CL + 1)), __uint_as_float(vload(e + W_CL + 2)));
-    s.mean_cosine = __uint_as_float(vload(e + W_CMEAN));
-    s.weight_sum = __uint_as_float(vload(e + W_CWS));
-    s.num_samples = vload(e + W_CNUM);
+    const uint2 a = vload2(e + W_CL), b = vload2(e + W_CL + 2), c = vload2(e + W_CWS);
+    s.light = mk(__uint_as_float(a.x), __uint_as_float(a.y), __uint_as_float(b.x));
+    s.mean_cosine = __uint_as_float(b.y);
+    s.weight_sum = __uint_as_float(c.x);
+    s.num_samples = c.y;
     s.score = __uint_as_float(vload(e + W_CSCORE));
     return s;
 }
@@ -151,10 +161,11 @@ LAM_DEV v3 grid_radiance(const Grid& g, v3 pos, v3 normal, v3 incoming) {
     IVec l = grid_loc(g, pos);
     uint64_t idx = primary_hash(l, normal, incoming) % g.len;
     uint32_t* e = g.world + idx * W_STRIDE;
-    uint32_t num = vload(e + W_NUM);
-    v3 rad = mk(__uint_as_float(vload(e + W_LUM)), __uint_as_float(vload(e + W_LUM + 1)), __uint_as_float(vload(e + W_LUM + 2)));
+    const uint2 sn = vload2(e + W_SEC), l01 = vload2(e + W_LUM);  // (tag, count), (radiance x, y)
+    uint32_t num = sn.y;
+    v3 rad = mk(__uint_as_float(l01.x), __uint_as_float(l01.y), __uint_as_float(vload(e + W_LUM + 2)));
     uint32_t sec = secondary_hash(l, normal);
-    if (vload(e + W_SEC) != sec) {
+    if (sn.x != sec) {
         const uint32_t* o = g.old_world ? g.old_world + idx * W_STRIDE : nullptr;
         if (o && vload(o + W_SEC) == sec) {
             num = vload(o + W_NUM);
