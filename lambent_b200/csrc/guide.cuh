@@ -108,6 +108,10 @@ LAM_DEV uint2 vload2(const uint32_t* p) {
     return v;
 }
 
+LAM_DEV void vstore2(uint32_t* p, uint32_t a, uint32_t b) {
+    asm volatile("st.volatile.global.v2.u32 [%0], {%1, %2};" ::"l"(p), "r"(a), "r"(b) : "memory");
+}
+
 LAM_DEV MC read_chain(const uint32_t* e) {
     MC s;
     const uint2 a = vload2(e + W_CL), b = vload2(e + W_CL + 2), c = vload2(e + W_CWS);
@@ -147,14 +151,10 @@ LAM_DEV void grid_store(const Grid& g, v3 pos, v3 normal, v3 incoming, const MC&
     if (vload(e + W_SEC) != sec) {
         if (atomicCAS(e + W_SEC, 0u, sec) != 0u) return;
     }
-    vstore(e + W_CL, __float_as_uint(st.light.x));
-    vstore(e + W_CL + 1, __float_as_uint(st.light.y));
-    vstore(e + W_CL + 2, __float_as_uint(st.light.z));
-    vstore(e + W_CMEAN, __float_as_uint(st.mean_cosine));
-    vstore(e + W_CWS, __float_as_uint(st.weight_sum));
-    vstore(e + W_CNUM, st.num_samples);
-    vstore(e + W_CSCORE, __float_as_uint(st.score));
-    vstore(e + W_TIMEOUT, CACHE_TIMEOUT);
+    vstore2(e + W_CL, __float_as_uint(st.light.x), __float_as_uint(st.light.y));
+    vstore2(e + W_CL + 2, __float_as_uint(st.light.z), __float_as_uint(st.mean_cosine));
+    vstore2(e + W_CWS, __float_as_uint(st.weight_sum), st.num_samples);
+    vstore2(e + W_CSCORE, __float_as_uint(st.score), CACHE_TIMEOUT);
 }
 
 LAM_DEV v3 grid_radiance(const Grid& g, v3 pos, v3 normal, v3 incoming) {
@@ -238,8 +238,10 @@ LAM_DEV void grid_add_radiance_warp(const Grid& g, v3 pos, v3 normal, v3 incomin
         if (ok) {
             __threadfence();
             num = vload(e + W_NUM);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) lum[k] = __uint_as_float(vload(e + W_LUM + k));
+            const uint2 l01 = vload2(e + W_LUM);
+            lum[0] = __uint_as_float(l01.x);
+            lum[1] = __uint_as_float(l01.y);
+            lum[2] = __uint_as_float(vload(e + W_LUM + 2));
         }
     }
     if (!__shfl_sync(grp, ok, leader)) return;
@@ -257,8 +259,8 @@ LAM_DEV void grid_add_radiance_warp(const Grid& g, v3 pos, v3 normal, v3 incomin
     if (lane == leader) {
         if (added) {
             atomicAdd(e + W_NUM, added);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) vstore(e + W_LUM + k, __float_as_uint(lum[k]));
+            vstore2(e + W_LUM, __float_as_uint(lum[0]), __float_as_uint(lum[1]));
+            vstore(e + W_LUM + 2, __float_as_uint(lum[2]));
         }
         __threadfence();
         atomicExch(e + W_LOCK, 0u);
