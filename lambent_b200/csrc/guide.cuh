@@ -123,18 +123,33 @@ LAM_DEV MC read_chain(const uint32_t* e) {
     return s;
 }
 
+// A cell's score and timeout words (the timeout is only ever set to CACHE_TIMEOUT while shading;
+// the end-of-frame pass lowers it).
+LAM_DEV MC read_chain_timeout(const uint32_t* e, uint32_t* timeout) {
+    MC s;
+    const uint2 a = vload2(e + W_CL), b = vload2(e + W_CL + 2), c = vload2(e + W_CWS), d = vload2(e + W_CSCORE);
+    s.light = mk(__uint_as_float(a.x), __uint_as_float(a.y), __uint_as_float(b.x));
+    s.mean_cosine = __uint_as_float(b.y);
+    s.weight_sum = __uint_as_float(c.x);
+    s.num_samples = c.y;
+    s.score = __uint_as_float(d.x);
+    *timeout = d.y;
+    return s;
+}
+
 LAM_DEV MC grid_load(const Grid& g, v3 pos, v3 normal, v3 incoming, bool force_old) {
     IVec l = grid_loc(g, pos);
     uint64_t idx = primary_hash(l, normal, incoming) % g.len;
     uint32_t* e = g.world + idx * W_STRIDE;
     uint32_t sec = secondary_hash(l, normal);
-    MC s = read_chain(e);
+    uint32_t timeout = 0u;
+    MC s = read_chain_timeout(e, &timeout);
     if (vload(e + W_SEC) != sec || force_old) {
         const uint32_t* o = g.old_world ? g.old_world + idx * W_STRIDE : nullptr;
         if (o && vload(o + W_SEC) == sec) s = read_chain(o);
         else s = mc_zero();
-    } else {
-        vstore(e + W_TIMEOUT, CACHE_TIMEOUT);
+    } else if (timeout != CACHE_TIMEOUT) {
+        vstore(e + W_TIMEOUT, CACHE_TIMEOUT);  // writing the value the word already holds is skipped
     }
     s.light = strip_nan3(s.light);
     s.mean_cosine = strip_nan(s.mean_cosine);
@@ -173,7 +188,7 @@ LAM_DEV v3 grid_radiance(const Grid& g, v3 pos, v3 normal, v3 incoming) {
         } else {
             return splat(0.0f);
         }
-    } else {
+    } else if (vload(e + W_TIMEOUT) != CACHE_TIMEOUT) {
         vstore(e + W_TIMEOUT, CACHE_TIMEOUT);
     }
     if (num == 0u) return splat(0.0f);
