@@ -362,6 +362,7 @@ LAM_DEV void screen_candidates(const Args& A, uint32_t pixel, uint32_t fill_seed
     const uint32_t sub = rand_u32(s) % 32u;
     MC sh = (gbase + sub < A.width) ? mc_load(A.tent_snap + (uint64_t)y * A.width + gbase + sub) : mc_zero();
     for (int i = 0; i < 4; ++i) cand[i] = sh;
+#pragma unroll 1
     for (int i = 4; i < 16; ++i) {
         uint32_t xr = rand_u32(s);
         s = xr;
@@ -400,7 +401,7 @@ template <int Q, bool GUIDE, bool LEARN, bool BATCH>
 // Six CTAs per SM for the unguided forms: the kernel waits on chains of dependent gathers (queue ->
 // hit -> triangle -> material -> texture), so resident warps matter more than the few registers
 // that spill (measured: 79 ms against 87 ms per 16-spp step at 1080p).  The Markov-guided form keeps
-// its registers (213 unbounded; 1 KB of spill at 80).
+// its registers (156 with its candidate loops rolled; 1 KB of spill at 80).
 __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(const __grid_constant__ Args A) {
     const uint32_t n = *A.count_in;
     const uint32_t lane = threadIdx.x & 31u;
@@ -563,6 +564,9 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 MC s = mc_zero();
                 if (GUIDE) {
                     screen_candidates(A, pixel, __float_as_uint(pn.w), cand);
+                    // the candidate loops stay rolled: the guided kernel is large, and unrolled it
+                    // needs 222 registers (2 CTAs per SM) and stalls on instruction fetch
+#pragma unroll 1
                     for (int k = 16; k < 20; ++k) {
                         bool rc = rand_f32(seed) < 0.7f;
                         float jm = rc ? 0.75f : 1.0f;
@@ -574,6 +578,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                     }
                     cand[20] = tentative;
                     sum_mc = 0.0f;
+#pragma unroll 1
                     for (int k = 0; k < NUM_RESAMPLES; ++k) {
                         seed = rand_u32(seed);
                         sum_mc += cand[k].weight_sum;
@@ -634,6 +639,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                         }
                         float mix_pdf = 0.0f;
                         if (GUIDE && c1 != 0.0f && sum_mc > 0.0f) {
+#pragma unroll 1
                             for (int k = 0; k < NUM_RESAMPLES; ++k) {
                                 if (!(cand[k].weight_sum > 0.0f)) continue;
                                 mix_pdf += vmf_pdf(normalize(light_dir(cand[k], ro)), get_kappa(cand[k]), dir) *
