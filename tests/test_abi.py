@@ -203,3 +203,11 @@ def test_layout_and_options():
     t.set_intersection_handler(None)
     with pytest.raises(lb.LambentError):
         lb.lib().lam_tracer_create(99, C.byref(C.c_void_p())) and lb.check(-1)
+
+
+def test_pipeline_tuning_entry_points_reject_null_pipelines():
+    """The host-side pipeline knobs validate their handle before anything touches the GPU."""
+    L = lb.lib()
+    assert L.lam_pipeline_set_wave_paths(None, C.c_uint64(1 << 20)) == _abi.ERR_INVALID_ARGUMENT
+    assert L.lam_pipeline_set_profiling(None, 1) == _abi.ERR_INVALID_ARGUMENT
+    assert L.lam_pipeline_set_guide(None, None) == _abi.ERR_INVALID_ARGUMENT
