@@ -487,28 +487,63 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
             MC tentative = GUIDE ? mc_load(A.tent_live + pixel) : mc_zero();
             const uint2 h = __ldg(A.hit + i);  // hits are stored by queue position (extend shares this queue)
             bool terminated = false;
-            if (h.x != NO_HIT) {
-                Isect is;
+            const bool hit = h.x != NO_HIT;
+            Isect is;
+            v3 new_pos, bg = splat(0.0f);
+            // what the chain updates take from either branch: radiance arriving at ro, its emitted
+            // part, and whether the previous direction came from the cosine lobe
+            v3 g_rad = splat(0.0f), g_out = splat(0.0f);
+            bool g_nvmf = false;
+            if (hit) {
                 make_isect(S, S.inst, h, make_float3(ro.x, ro.y, ro.z), make_float3(rd.x, rd.y, rd.z), is, A.phit_a,
                            A.phit_b, path);
-                v3 new_pos = fma3(rd, splat(is.t), ro);
+                new_pos = fma3(rd, splat(is.t), ro);
                 if (depth != 0u) {
                     v3 est = GUIDE ? grid_radiance(G, new_pos, is.normal, rd) : splat(0.0f);
                     v3 rad_refl = strip_nan3(((is.color * est) * cached_brdf) / cached_pdf);
                     v3 rad_out = (is.emission * cached_brdf) / cached_pdf;
-                    if (GUIDE) grid_add_radiance_warp(G, ro, last_normal, last_dir, rad_out + rad_refl);
-                    float weight = len(rad_out + rad_refl);
-                    if (weight > 0.0f) {
-                        if (GUIDE) {
-                            MC st = update_chain(ro, new_pos, weight, seed, false, grid_load(G, ro, last_normal, last_dir, false),
-                                                 1.0f, sum_mc);
-                            grid_store_warp(G, ro, last_normal, last_dir, st);
-                            tentative = update_chain(ro, new_pos, len(rad_out), seed, last_not_vmf, tentative,
-                                                     depth == 1u ? 1.0f : 0.5f, sum_mc);
-                        }
-                        seed++;
+                    g_rad = rad_out + rad_refl;
+                    g_out = rad_out;
+                    g_nvmf = last_not_vmf;
+                }
+            } else {
+                bg = sky_sample(S, rd);
+                new_pos = fma3(rd, splat(A.tmax), ro);
+                if (depth == 1u && rec) {
+                    A.vpoint[path] = make_float4(new_pos.x, new_pos.y, new_pos.z, 0.0f);
+                    A.vnormal[path] = make_float4(-rd.x, -rd.y, -rd.z, 0.0f);
+                }
+                if (depth == 0u && last_sample) {
+                    if (out_normal) out_normal[pixel] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+                    if (out_albedo) out_albedo[pixel] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+                    if (A.pix_emission) {
+                        A.pix_emission[pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        A.pix_albedo[pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                     }
                 }
+                if (depth != 0u) {
+                    orad = fma3(orc, bg, orad);
+                    g_rad = (bg * cached_brdf) / cached_pdf;
+                    g_out = g_rad;
+                }
+            }
+            // one call site for the chain updates of hit and sky lanes (general.wesl:677-684 and
+            // :928-935 run the same updates), so a warp with both kinds runs them once
+            if (depth != 0u) {
+                if (GUIDE) grid_add_radiance_warp(G, ro, last_normal, last_dir, g_rad);
+                float weight = len(g_rad);
+                if (weight > 0.0f) {
+                    if (GUIDE) {
+                        MC st = update_chain(ro, new_pos, weight, seed, false, grid_load(G, ro, last_normal, last_dir, false),
+                                             1.0f, sum_mc);
+                        grid_store_warp(G, ro, last_normal, last_dir, st);
+                        tentative = update_chain(ro, new_pos, len(g_out), seed, g_nvmf, tentative,
+                                                 depth == 1u ? 1.0f : 0.5f, sum_mc);
+                    }
+                    seed++;
+                }
+            }
+            if (hit) {
                 last_normal = is.normal;
                 last_dir = rd;
                 last_not_vmf = false;
@@ -668,36 +703,6 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 cont = depth + 1u < A.max_depth;
                 terminated = !cont;
             } else {
-                v3 bg = sky_sample(S, rd);
-                v3 new_pos = fma3(rd, splat(A.tmax), ro);
-                if (depth == 1u && rec) {
-                    A.vpoint[path] = make_float4(new_pos.x, new_pos.y, new_pos.z, 0.0f);
-                    A.vnormal[path] = make_float4(-rd.x, -rd.y, -rd.z, 0.0f);
-                }
-                if (depth == 0u && last_sample) {
-                    if (out_normal) out_normal[pixel] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-                    if (out_albedo) out_albedo[pixel] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-                    if (A.pix_emission) {
-                        A.pix_emission[pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                        A.pix_albedo[pixel] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                    }
-                }
-                if (depth != 0u) {
-                    orad = fma3(orc, bg, orad);
-                    v3 rad_out = (bg * cached_brdf) / cached_pdf;
-                    if (GUIDE) grid_add_radiance_warp(G, ro, last_normal, last_dir, rad_out);
-                    float weight = len(rad_out);
-                    if (weight > 0.0f) {
-                        if (GUIDE) {
-                            MC st = update_chain(ro, new_pos, weight, seed, false, grid_load(G, ro, last_normal, last_dir, false),
-                                                 1.0f, sum_mc);
-                            grid_store_warp(G, ro, last_normal, last_dir, st);
-                            tentative = update_chain(ro, new_pos, len(rad_out), seed, false, tentative,
-                                                     depth == 1u ? 1.0f : 0.5f, sum_mc);
-                        }
-                        seed++;
-                    }
-                }
                 scol = fma3(color, bg, scol);
                 terminated = true;
             }
