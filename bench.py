@@ -137,17 +137,27 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def build_scene(a):
+def build_scene(a, packer=None):
     from lambent_b200 import scenes
-    return scenes.icosphere_field(a.width, a.height, instances=a.instances, subdiv=a.subdiv, tex_size=a.tex)
+    return scenes.icosphere_field(a.width, a.height, instances=a.instances, subdiv=a.subdiv, tex_size=a.tex,
+                                  packer=packer)
 
 
-def cpu_reference(a, scene, seconds):
+def oracle_scene(a):
+    """The workload's scene with its material records and camera packed by the oracle's own
+    restatements of Material::new and Camera::from_proj_view: the CPU legs load no product code."""
+    from oracle import oracle_py as O
+    return build_scene(a, packer=O.OraclePacker)
+
+
+def cpu_reference(a, seconds, scene=None):
     """The reference path on the host cores: the CPU restatement of its shaders, a crop of the
     same frame (full-frame rays and seeds) sized to about `seconds` of work."""
     from oracle import oracle_py as O
     from lambent_b200 import _abi
     cores = os.cpu_count() or 1
+    if scene is None:
+        scene = oracle_scene(a)
     osc = O.OracleScene(scene)
     w = h = min(128, min(a.width, a.height)) // 32 * 32  # calibration crop
     x0, y0 = a.width // 2 - w // 2, a.height // 2 - h // 2
@@ -177,8 +187,8 @@ def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    scene = build_scene(a)
-    base = cpu_reference(a, scene, a.cpu_seconds)
+    scene = oracle_scene(a)
+    base = cpu_reference(a, a.cpu_seconds, scene)
     steps_ms = []
     # each step is a bounded sample of the workload; value = Mrays/s over the steps
     from oracle import oracle_py as O
@@ -545,14 +555,18 @@ def run_ours(a):
     normal = torch.zeros_like(color)
     albedo = torch.zeros_like(color)
     tg = lb.targets_from(color, normal, albedo)
-    seed0 = rank * 1_000_003
+    from lambent_b200 import distributed as D
 
+    # seeds: step k of this rank renders with D.rank_seed(0, rank, k), disjoint from every other rank
     for k in range(a.warmup):
-        pipe.render(gscene, bufs, scene.camera, tg, seed0 + k, stream)
+        pipe.render(gscene, bufs, scene.camera, tg, D.rank_seed(0, rank, k), stream)
     torch.cuda.synchronize()
     pipe.set_profiling(True)
     pipe.profile_reset()
-    accum = torch.zeros_like(color)
+
+    def frame(seed):
+        pipe.render(gscene, bufs, scene.camera, tg, seed, stream)
+        return color
 
     def barrier():
         if world > 1:
@@ -563,11 +577,8 @@ def run_ours(a):
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(torch.cuda.current_device()) as clocks:
         start.record(stream)
-        for k in range(a.steps):
-            pipe.render(gscene, bufs, scene.camera, tg, seed0 + a.warmup + k, stream)
-            accum.add_(color)
-        if world > 1:
-            dist.all_reduce(accum)
+        # sample sharding: the per-rank sum of the steps' frames, one all-reduce at the end
+        D.render_sharded(frame, a.steps, first_step=a.warmup)
         end.record(stream)
         torch.cuda.synchronize()
     barrier()
@@ -587,12 +598,10 @@ def run_ours(a):
         ms_max, segs_total = ms, float(segs)
     value = segs_total / (ms_max / 1e3) / 1e6
 
-    # e2e through the public API with host buffers: camera H2D + render + colour D2H per step.  Two
-    # target sets: frame k's readback (on a copy stream) overlaps frame k+1's render, and a target is
-    # rendered into again only after its previous readback has finished.
-    pinned_cam = torch.empty(32, dtype=torch.float32).pin_memory()
-    pinned_cam.copy_(torch.tensor(list(scene.camera.c.projection_inverse) + list(scene.camera.c.view_inverse)))
-    cam_dev = torch.empty(32, dtype=torch.float32, device=dev)
+    # e2e through the public API with host buffers: render + colour D2H per step.  The step's input is
+    # the 128-byte camera, a host record that lam_render passes by value to its launches.  Two target
+    # sets: frame k's readback (on a copy stream) overlaps frame k+1's render, and a target is rendered
+    # into again only after its previous readback has finished.
     colors = [color, torch.zeros_like(color)]
     tgs = [tg, lb.targets_from(colors[1], torch.zeros_like(color), torch.zeros_like(color))]
     host_imgs = [torch.empty((H, W, 4), dtype=torch.float32).pin_memory() for _ in range(2)]
@@ -609,8 +618,7 @@ def run_ours(a):
         b = k % 2
         if k >= 2:
             stream.wait_event(copied[b])
-        cam_dev.copy_(pinned_cam, non_blocking=True)
-        pipe.render(gscene, bufs, scene.camera, tgs[b], seed0 + 7777 + k, stream)
+        pipe.render(gscene, bufs, scene.camera, tgs[b], D.rank_seed(0, rank, a.warmup + a.steps + k), stream)
         rendered[b].record(stream)
         copy_stream.wait_event(rendered[b])
         with torch.cuda.stream(copy_stream):
@@ -664,7 +672,9 @@ def run_ours(a):
                                       "achieved": round(value / world * 1e6 * SEG_BYTES_TOTAL / 1e9, 2),
                                       "frac": round(value / world * 1e6 * SEG_BYTES_TOTAL / 1e9 / hbm, 5)}},
             "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 128,
-                    "d2h_bytes_per_step": H * W * 16},
+                    "d2h_bytes_per_step": H * W * 16,
+                    "note": "per step: the 128-B host camera record passed by value into lam_render's launches, "
+                            "and the rgba32f colour image read back to pinned host memory"},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "scene": {"triangles": st.triangle_count, "blas_nodes": st.blas_node_count,
@@ -672,7 +682,7 @@ def run_ours(a):
                       "build_s": round(st.build_seconds, 3)},
         }
         if not a.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_reference(a, scene, a.cpu_seconds)
+            line["cpu_baseline"] = cpu_reference(a, a.cpu_seconds)
         if world == 1 and not (a.no_guided and a.no_batched and a.no_restir):
             del gscene, pipe, bufs
             torch.cuda.empty_cache()

@@ -405,7 +405,10 @@ int lam_scene_stats_get(const lam_scene* scene, lam_scene_stats* out);
 int lam_scene_destroy(lam_scene* scene);
 
 /* Ray-query closest hit / any hit (rayQueryInitialize..GetCommittedIntersection,
- * general.wesl:1053-1078) for n rays held in device memory. */
+ * general.wesl:1053-1078) for n rays held in device memory.  n <= LAM_TRACE_MAX_RAYS, and the
+ * current device must be the scene's (LAM_ERR_INVALID_ARGUMENT otherwise).  The call waits for
+ * its stream before it returns. */
+#define LAM_TRACE_MAX_RAYS 0x7FFFFFFFu
 int lam_trace_rays(const lam_scene* scene, const lam_ray* rays, uint32_t n, uint32_t mode,
                    lam_hit* hits, void* stream);
 
@@ -424,8 +427,11 @@ int lam_pipeline_trace_rays(lam_pipeline* pipeline, const lam_scene* scene, cons
  * static device array that every GPU loading this library keeps until the process exits.
  * n must not exceed LAM_TRACE_STATIC_MAX_RAYS (larger n: LAM_ERR_INVALID_ARGUMENT).  All calls
  * share that array: calls that overlap on the GPU race and must be serialised.  The first call on
- * a device looks up the array's device address; make it before any stream capture.  The current
- * device must be the scene's.  Results are identical to lam_trace_rays. */
+ * a device looks up the array's device address (in the CUDA runtime's primary context) and keeps
+ * it for the life of the process; make that first call before any stream capture, and do not use
+ * this entry point across cudaDeviceReset, which leaves the kept address stale.  Each call reads
+ * the error flags back and waits for its stream before it returns.  The current device must be the
+ * scene's.  Results are identical to lam_trace_rays. */
 #define LAM_TRACE_STATIC_MAX_RAYS 0x7FFFFFFFu
 int lam_trace_rays_static(const lam_scene* scene, const lam_ray* rays, uint32_t n, uint32_t mode,
                           lam_hit* hits, void* stream);

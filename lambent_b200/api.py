@@ -431,8 +431,10 @@ class Pipeline:
         check(lib().lam_render_profile_reset(self._h))
 
     def trace_rays(self, scene, rays, hits, mode=_abi.TRACE_CLOSEST, stream=None):
-        """lam_pipeline_trace_rays: ray queries that run the pipeline's intersection handler."""
-        check(lib().lam_pipeline_trace_rays(self._h, scene._h, C.c_void_p(rays.data_ptr()), rays.shape[0], mode,
+        """lam_pipeline_trace_rays: ray queries that run the pipeline's intersection handler.
+        rays / hits as for GpuScene.trace."""
+        n = _check_ray_tensors(scene, rays, hits)
+        check(lib().lam_pipeline_trace_rays(self._h, scene._h, C.c_void_p(rays.data_ptr()), n, mode,
                                             C.c_void_p(hits.data_ptr()), _stream_ptr(stream)))
 
     def batch_render(self, requests, tuning=None, stream=None):
@@ -487,6 +489,8 @@ class GpuScene:
         check(lib().lam_scene_create(self.holder.ptr(), _stream_ptr(stream), C.byref(h)))
         self._h = h
         self.holder = None
+        import torch
+        self.device = torch.device("cuda", torch.cuda.current_device())  # the scene lives on this device
 
     def stats(self):
         s = SceneStats()
@@ -504,8 +508,10 @@ class GpuScene:
         check(lib().lam_scene_update_materials(self._h, arr, len(materials), _stream_ptr(stream)))
 
     def trace(self, rays, hits, mode=_abi.TRACE_CLOSEST, stream=None):
-        """rays: CUDA tensor (n, 8) float32; hits: CUDA tensor (n, 6) int32/float32 storage (24 B each)."""
-        n = rays.shape[0]
+        """rays: contiguous CUDA tensor (n, 8) float32 on the scene's device (lam_ray records); hits:
+        contiguous CUDA tensor of at least n rows of 6 four-byte elements (int32 / uint32 / float32
+        storage of lam_hit records).  Anything else raises ValueError before the C-ABI is called."""
+        n = _check_ray_tensors(self, rays, hits)
         check(lib().lam_trace_rays(self._h, C.c_void_p(rays.data_ptr()), n, mode, C.c_void_p(hits.data_ptr()),
                                    _stream_ptr(stream)))
 
@@ -513,6 +519,32 @@ class GpuScene:
         if getattr(self, "_h", None) and _LIB is not None:
             _LIB.lam_scene_destroy(self._h)
             self._h = None
+
+
+def _check_ray_tensors(scene, rays, hits):
+    """Validates the ray / hit tensors of a ray query and returns the ray count: the kernels read
+    32-byte rays and write 24-byte hits through raw device pointers, so a host tensor, a strided view,
+    a wrong element size or a short hit tensor would make them access memory out of bounds."""
+    import torch
+    for name, t in (("rays", rays), ("hits", hits)):
+        if not isinstance(t, torch.Tensor) or not t.is_cuda:
+            raise ValueError(f"{name} must be a CUDA tensor")
+        if t.device != scene.device:
+            raise ValueError(f"{name} is on {t.device}, the scene on {scene.device}")
+        if not t.is_contiguous():
+            raise ValueError(f"{name} must be contiguous")
+    if rays.dtype != torch.float32 or rays.dim() != 2 or rays.shape[1] != 8:
+        raise ValueError("rays must be a float32 tensor of shape (n, 8)")
+    if hits.dtype not in (torch.int32, torch.float32) and str(hits.dtype) != "torch.uint32":
+        raise ValueError("hits must hold 4-byte elements (int32, uint32 or float32)")
+    if hits.dim() != 2 or hits.shape[1] != 6:
+        raise ValueError("hits must have shape (m, 6)")
+    n = rays.shape[0]
+    if hits.shape[0] < n:
+        raise ValueError(f"hits holds {hits.shape[0]} rows, fewer than the {n} rays")
+    if n > 0xFFFFFFFF:
+        raise ValueError("too many rays for one query")
+    return n
 
 
 # ---------------------------------------------------------------- DataBuffers (src/data_buffer/mod.rs)

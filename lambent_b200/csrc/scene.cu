@@ -428,6 +428,17 @@ __global__ void __launch_bounds__(TRACE_BLOCK) trace_rays_kernel(DevScene S, con
     if (err) atomicOr(err_out, err);
 }
 
+int check_trace_call(const lam_scene* s, uint32_t n, const char* who) {
+    if (n > LAM_TRACE_MAX_RAYS)
+        return set_error(LAM_ERR_INVALID_ARGUMENT, std::string(who) + ": n exceeds LAM_TRACE_MAX_RAYS (2^31 - 1)");
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return cuda_error(e, who);
+    if (device != s->device)
+        return set_error(LAM_ERR_INVALID_ARGUMENT, std::string(who) + ": the current device is not the scene's");
+    return LAM_OK;
+}
+
 }  // namespace lam
 
 extern "C" int lam_trace_rays(const lam_scene* s, const lam_ray* rays, uint32_t n, uint32_t mode, lam_hit* hits,
@@ -436,6 +447,7 @@ extern "C" int lam_trace_rays(const lam_scene* s, const lam_ray* rays, uint32_t 
     if (mode != LAM_TRACE_CLOSEST && mode != LAM_TRACE_ANY)
         return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_trace_rays: unknown mode");
     if (n == 0) return LAM_OK;
+    if (int rc = check_trace_call(s, n, "lam_trace_rays")) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     uint32_t* scratch = nullptr;  // [0] work counter, [1] error flags
     cudaError_t e = cudaMallocAsync((void**)&scratch, 8, st);
@@ -483,7 +495,10 @@ extern "C" int lam_trace_rays(const lam_scene* s, const lam_ray* rays, uint32_t 
 //     several host threads) race on the counter and give wrong results; serialise them;
 //   * the array keeps the last call's contents; each call clears the two words it uses first;
 //   * the first call on a device resolves the array's device address with cudaGetSymbolAddress
-//     (once per device); make that first call before any stream capture.
+//     (once per device, in the CUDA runtime's primary context of that device) and keeps it for the
+//     life of the process; make that first call before any stream capture.  After cudaDeviceReset
+//     the kept address is stale, so the entry point must not be used across a device reset;
+//   * every call reads the error flags back and synchronises its stream before it returns.
 namespace lam {
 
 constexpr uint32_t STATIC_TRACE_WORDS = 64;  // 256 bytes; words 0 (work counter) and 1 (error flags) used

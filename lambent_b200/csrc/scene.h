@@ -67,4 +67,8 @@ namespace lam {
 // thread-local error reporting shared by all translation units
 int set_error(int code, const std::string& msg);
 int cuda_error(cudaError_t e, const char* what);
+// Checks shared by the ray-query entry points: n within LAM_TRACE_MAX_RAYS (the 32-bit work counter
+// overshoots n by at most one claim per warp of the grid and must not wrap) and the current device
+// being the scene's (the kernels dereference the scene's device pointers).
+int check_trace_call(const lam_scene* s, uint32_t n, const char* who);
 }  // namespace lam

@@ -2194,6 +2194,7 @@ extern "C" int lam_pipeline_trace_rays(lam_pipeline* pl, const lam_scene* s, con
     if (mode != LAM_TRACE_CLOSEST && mode != LAM_TRACE_ANY)
         return set_error(LAM_ERR_INVALID_ARGUMENT, "lam_pipeline_trace_rays: unknown mode");
     if (n == 0) return LAM_OK;
+    if (int rc = check_trace_call(s, n, "lam_pipeline_trace_rays")) return rc;
     int rc = ensure_handler(pl);
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;

@@ -27,12 +27,16 @@ def combine(sum_image, frames_per_rank, group=None):
     return out / float(frames_per_rank * world)
 
 
-def render_sharded(render_frame, frames, base_seed=0, group=None):
-    """render_frame(seed) -> image tensor; renders `frames` frames on this rank and returns the
-    mean over all ranks' frames."""
+def render_sharded(render_frame, frames, base_seed=0, group=None, first_step=0):
+    """render_frame(seed) -> image tensor; renders `frames` frames on this rank (steps first_step ..
+    first_step + frames - 1 of its seed range) and returns the mean over all ranks' frames.  The
+    per-rank sum is accumulated in place, and the ranks exchange it once, at the end."""
     rank = dist.get_rank(group) if dist.is_initialized() else 0
     acc = None
     for k in range(frames):
-        img = render_frame(rank_seed(base_seed, rank, k))
-        acc = img.clone() if acc is None else acc + img
+        img = render_frame(rank_seed(base_seed, rank, first_step + k))
+        if acc is None:
+            acc = img.clone()
+        else:
+            acc.add_(img)
     return combine(acc, frames, group)

@@ -10,8 +10,10 @@
   occluded_cornell()    indirect-heavy: the Cornell box lit by one 0.2 x 0.2 emitter behind an occluder.
   box_field(n_tris)     batched requests: Cornell-style scenes with n_tris triangles of subdivided boxes.
 
-Cameras follow cgmath's perspective / look_to_rh conventions (examples/cornell_box/src/main.rs:500-507)
-and materials are packed through the library's Material::new.
+Cameras follow cgmath's perspective / look_to_rh conventions (examples/cornell_box/src/main.rs:500-507).
+Material records and cameras are packed by a packer: by default the library's Material::new and
+Camera::from_proj_view (LibraryPacker); any object with the same two methods can stand in for it, so
+that a scene can be generated without loading the library at all.
 """
 import math
 
@@ -40,6 +42,23 @@ class Scene:
     def layout_counts(self):
         return (max(1, len(self.instances)), max(1, len(self.diffuse)), max(1, len(self.emission)),
                 max(1, len(self.attributes)))
+
+
+class LibraryPacker:
+    """Packs through the library: Material::new (src/lib.rs:132-163) and Camera::from_proj_view
+    (src/camera.rs:15-24)."""
+
+    @staticmethod
+    def material(uv1, uv2, uv3, recolour, diffuse, emission, attributes, emission_scale, ior, ty):
+        return Material.new(uv1, uv2, uv3, recolour, diffuse, emission, attributes, emission_scale, ior, ty)
+
+    @staticmethod
+    def camera(proj, view):
+        return Camera.new(proj, view)
+
+
+def _packer(packer):
+    return LibraryPacker if packer is None else packer
 
 
 IDENTITY = np.array([1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0], dtype=np.float32)
@@ -72,9 +91,10 @@ def look_to_rh(eye, direction, up):
     return m.astype(np.float32)
 
 
-def make_camera(eye, target, fovy_deg, aspect, up=(0.0, 1.0, 0.0)):
+def make_camera(eye, target, fovy_deg, aspect, up=(0.0, 1.0, 0.0), packer=None):
     d = np.asarray(target, np.float64) - np.asarray(eye, np.float64)
-    return Camera.new(perspective(fovy_deg, aspect, 0.1, 200.0), look_to_rh(eye, d, np.asarray(up, np.float64)))
+    return _packer(packer).camera(perspective(fovy_deg, aspect, 0.1, 200.0),
+                                  look_to_rh(eye, d, np.asarray(up, np.float64)))
 
 
 def solid(rgba, size=64):
@@ -84,9 +104,9 @@ def solid(rgba, size=64):
 UV = ((1.0, 1.0), (0.0, 1.0), (1.0, 0.0))
 
 
-def _mat(diffuse, emission=None, attributes=None, scale=1.0, ior=None, ty=MaterialType.Diffuse, uv=UV):
-    return Material.new(uv[0], uv[1], uv[2], (0, 0), diffuse, emission, attributes,
-                        EmissionScale.from_emission_scale(scale), ior, ty)
+def _mat(diffuse, emission=None, attributes=None, scale=1.0, ior=None, ty=MaterialType.Diffuse, uv=UV, packer=None):
+    return _packer(packer).material(uv[0], uv[1], uv[2], (0, 0), diffuse, emission, attributes,
+                                    EmissionScale.from_emission_scale(scale), ior, ty)
 
 
 def _quad(p0, p1, p2, p3):
@@ -116,7 +136,7 @@ def _box(center, size, angle_deg):
     return tris
 
 
-def cornell_box(width=256, height=256, light_size=0.5, light_emission=15.0, occluder=False):
+def cornell_box(width=256, height=256, light_size=0.5, light_emission=15.0, occluder=False, packer=None):
     """The procedural Cornell box (36 triangles; 48 with the occluder variant)."""
     s = Scene()
     s.name = "cornell_box"
@@ -160,17 +180,17 @@ def cornell_box(width=256, height=256, light_size=0.5, light_emission=15.0, occl
     s.emission = [solid((255, 255, 255, 255))]
     s.attributes = [solid((77, 77, 0, 0))]  # roughness 0.3 in x/y
     s.materials = [
-        _mat(0), _mat(1), _mat(2),
-        _mat(3, emission=0, scale=light_emission if not occluder else light_emission * 6.25),
-        _mat(0, attributes=0, ty=MaterialType.Metallic),
-        _mat(3, ior=(1.5, 1.5), ty=MaterialType.Transparent),
+        _mat(0, packer=packer), _mat(1, packer=packer), _mat(2, packer=packer),
+        _mat(3, emission=0, scale=light_emission if not occluder else light_emission * 6.25, packer=packer),
+        _mat(0, attributes=0, ty=MaterialType.Metallic, packer=packer),
+        _mat(3, ior=(1.5, 1.5), ty=MaterialType.Transparent, packer=packer),
     ]
-    s.camera = make_camera((0.0, 1.0, 3.4), (0.0, 1.0, 0.0), 40.0, width / height)
+    s.camera = make_camera((0.0, 1.0, 3.4), (0.0, 1.0, 0.0), 40.0, width / height, packer=packer)
     return s
 
 
-def occluded_cornell(width=256, height=256):
-    return cornell_box(width, height, light_size=0.2, occluder=True)
+def occluded_cornell(width=256, height=256, packer=None):
+    return cornell_box(width, height, light_size=0.2, occluder=True, packer=packer)
 
 
 # ---------------------------------------------------------------- icospheres
@@ -235,7 +255,8 @@ def value_noise(rng, size, octaves=4, base=8, channels=4):
     return np.ascontiguousarray((out / total).transpose(1, 2, 0))
 
 
-def icosphere_field(width=1920, height=1080, instances=64, subdiv=5, tex_size=1024, tex_layers=16, seed=2024):
+def icosphere_field(width=1920, height=1080, instances=64, subdiv=5, tex_size=1024, tex_layers=16, seed=2024,
+                    packer=None):
     rng = np.random.default_rng(seed)
     s = Scene()
     s.name = f"icosphere_field_{instances}x{20 * 4 ** subdiv}"
@@ -285,7 +306,8 @@ def icosphere_field(width=1920, height=1080, instances=64, subdiv=5, tex_size=10
         a_layer = int(rng.integers(tex_layers))
         for _ in range(n_variants):
             uv = tuple(tuple(float(x) for x in rng.random(2)) for _ in range(3))
-            s.materials.append(_mat(d_layer, emission=emis, attributes=a_layer, scale=scale, ior=ior, ty=ty, uv=uv))
+            s.materials.append(_mat(d_layer, emission=emis, attributes=a_layer, scale=scale, ior=ior, ty=ty, uv=uv,
+                                    packer=packer))
         h = (np.arange(ntri, dtype=np.uint64) * np.uint64(2654435761) + np.uint64(i)) % np.uint64(n_variants)
         s.instances.append({"transform": xf, "blas": i, "material_indices": (first + h).astype(np.uint32)})
     # sky: vertical gradient on all six faces (bright above, dark below)
@@ -304,14 +326,14 @@ def icosphere_field(width=1920, height=1080, instances=64, subdiv=5, tex_size=10
         faces_img[fidx, ..., :3] = (np.clip(img, 0, 1) * 255).astype(np.uint8)
         faces_img[fidx, ..., 3] = 255
     s.sky = faces_img
-    s.camera = make_camera((0.0, 2.0, 16.0), (0.0, 0.0, 0.0), 55.0, width / height)
+    s.camera = make_camera((0.0, 2.0, 16.0), (0.0, 0.0, 0.0), 55.0, width / height, packer=packer)
     return s
 
 
-def box_field(n_tris, width=512, height=512, seed=0):
+def box_field(n_tris, width=512, height=512, seed=0, packer=None):
     """Cornell box plus subdivided boxes filling it up to about n_tris triangles (batched requests)."""
     rng = np.random.default_rng(seed)
-    s = cornell_box(width, height)
+    s = cornell_box(width, height, packer=packer)
     s.name = f"box_field_{n_tris}"
     v = [s.blas[0]["vertices"]]
     mats = [s.instances[0]["material_indices"]]
@@ -336,7 +358,7 @@ def box_field(n_tris, width=512, height=512, seed=0):
     return s
 
 
-def unit_cube_scene(width=128, height=128):
+def unit_cube_scene(width=128, height=128, packer=None):
     """The reference test's unit-cube geometry (src/tests/mod.rs:52-167): 8 vertices, 8 triangles."""
     s = Scene()
     s.name = "unit_cube"
@@ -354,11 +376,12 @@ def unit_cube_scene(width=128, height=128):
             (P[1], P[0], P[3], 0, 0, 0, None, 1), (P[0], P[1], P[2], 1, None, None, W, 2),
             (P[1], P[3], P[2], 1, None, None, W, 2)]
     for a, b, c, d, e, att, ior, ty in spec:
-        s.materials.append(Material.new(a, b, c, (0, 0), d, e, att, EmissionScale.from_emission_scale(1.0), ior, ty))
+        s.materials.append(_packer(packer).material(a, b, c, (0, 0), d, e, att, EmissionScale.from_emission_scale(1.0),
+                                                    ior, ty))
     s.diffuse = [solid((34, 177, 76, 255)), solid((250, 250, 250, 255))]
     s.emission = [solid((255, 0, 0, 255)), solid((0, 0, 0, 255))]
     s.attributes = [solid((20, 20, 0, 255))]
-    s.camera = make_camera((2.5, 2.0, 2.5), (0.5, 0.5, 0.5), 45.0, width / height)
+    s.camera = make_camera((2.5, 2.0, 2.5), (0.5, 0.5, 0.5), 45.0, width / height, packer=packer)
     return s
 
 

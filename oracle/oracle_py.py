@@ -83,6 +83,40 @@ def lib():
     return L
 
 
+class OracleCamera:
+    """A packed camera record (`.c`, the 128-byte lam_camera) made without the product library."""
+
+    def __init__(self, c):
+        self.c = c
+
+
+class OraclePacker:
+    """Scene packer for lambent_b200.scenes that uses the oracle's own restatements of
+    Material::new (src/lib.rs:132-163) and Camera::from_proj_view (src/camera.rs:15-24, 59-70), so
+    that the CPU legs of the benchmark never load the product library."""
+
+    @staticmethod
+    def material(uv1, uv2, uv3, recolour, diffuse, emission, attributes, emission_scale, ior, ty):
+        f2 = lambda p: (C.c_float * 2)(*p)
+        m = _abi.Material()
+        rc = lib().oracle_material_new(f2(uv1), f2(uv2), f2(uv3), (C.c_uint16 * 2)(*recolour), diffuse,
+                                       -1 if emission is None else emission, -1 if attributes is None else attributes,
+                                       emission_scale.emissive_texture_scale, emission_scale.diffuse_texture_scale,
+                                       None if ior is None else f2(ior), ty, C.byref(m))
+        if rc != 0:
+            raise ValueError(f"oracle_material_new failed: {rc}")
+        return m
+
+    @staticmethod
+    def camera(proj, view):
+        flat = lambda m: (C.c_float * 16)(*[float(x) for x in np.asarray(m, np.float32).reshape(-1)])
+        c = _abi.Camera()
+        rc = lib().oracle_camera_from_proj_view(flat(proj), flat(view), C.byref(c))
+        if rc != 0:
+            raise ValueError(f"oracle_camera_from_proj_view failed: {rc}")
+        return OracleCamera(c)
+
+
 HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("prim", "<u4"), ("inst", "<u4"), ("kind", "<u4")])
 
 

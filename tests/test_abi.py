@@ -176,10 +176,13 @@ def test_texture_loader_raw_cuboids_and_errors():
         tl.load("/nonexistent/texture.png")
 
 
-REF_PNG = "/root/reference/src/tests"
+# The reference checkout's root, when one is available (LAMBENT_REFERENCE_DIR); its 64x64 PNG
+# fixtures live under src/tests.
+REF_PNG = os.path.join(os.environ.get("LAMBENT_REFERENCE_DIR", ""), "src", "tests")
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_PNG), reason="reference fixtures not mounted")
+@pytest.mark.skipif(not os.environ.get("LAMBENT_REFERENCE_DIR") or not os.path.isdir(REF_PNG),
+                    reason="set LAMBENT_REFERENCE_DIR to a reference checkout to decode its PNG fixtures")
 def test_texture_loader_reads_reference_fixtures():
     # first pixels as recorded for the reference's own 64x64 RGBA8 fixtures
     tl = lb.TextureLoader()

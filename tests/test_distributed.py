@@ -62,3 +62,33 @@ def test_rank_seed_range():
     assert D.rank_seed(0, 1, 0) == D.SEED_STRIDE
     with pytest.raises(ValueError):
         D.rank_seed(0, 0, D.SEED_STRIDE)
+
+
+def _worker_offset(rank, world, port, out_dir):
+    """render_sharded with first_step: the seeds continue the rank's range after the warm-up steps,
+    as bench.py's timed loop uses them."""
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    seeds = []
+
+    def frame(seed):
+        seeds.append(seed)
+        return torch.full((4, 4), float(seed % 97), dtype=torch.float64)
+
+    img = D.render_sharded(frame, 3, first_step=2)
+    np.save(os.path.join(out_dir, f"img{rank}.npy"), img.numpy())
+    np.save(os.path.join(out_dir, f"seeds{rank}.npy"), np.array(seeds))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_sharding_after_warmup(tmp_path):
+    world = 2
+    mp.start_processes(_worker_offset, args=(world, _free_port(), str(tmp_path)), nprocs=world, start_method="spawn")
+    seeds = [np.load(tmp_path / f"seeds{r}.npy").tolist() for r in range(world)]
+    assert seeds == [[D.rank_seed(0, r, k) for k in (2, 3, 4)] for r in range(world)]
+    want = np.mean([s % 97 for r in range(world) for s in seeds[r]])
+    for r in range(world):
+        np.testing.assert_allclose(np.load(tmp_path / f"img{r}.npy"), np.full((4, 4), want))
