@@ -69,6 +69,10 @@ def parse():
     p.add_argument("--no-restir", action="store_true", help="skip the ReSTIR GI frame-loop measurement")
     p.add_argument("--restir-only", action="store_true", help="run only the ReSTIR GI frame-loop measurement")
     p.add_argument("--restir-frames", type=int, default=120)
+    p.add_argument("--restir-ref-spp", type=int, default=4096,
+                   help="spp of the plain reference of each compared ReSTIR frame (two independent halves)")
+    p.add_argument("--restir-compare", default="29,59,89,119",
+                   help="orbit frames whose ReSTIR output is compared with plain path tracing at equal time")
     p.add_argument("--batched-only", action="store_true", help="run only the batched-serving measurement")
     p.add_argument("--batched-requests", type=int, default=64)
     p.add_argument("--batched-scenes", type=int, default=8, help="distinct scenes shared by the requests")
@@ -423,13 +427,89 @@ def restir_frames(a, dev):
     pipe.set_profiling(False)
     assert pipe.stats().error_flags == 0, "ReSTIR frame loop reported an error"
     n = a.restir_frames
+    equal_time = restir_equal_time(a, dev, s, gs, pipe, col, tg, cams, ms / n)
     return {"config": {"workload": f"Cornell box (36 tris), {W}x{H}, {n}-frame orbit, 1 spp/frame, depth 8, "
                                    "Medium, per-pixel reservoirs, Markov chains (1.5M world cells), temporal + "
                                    "spatial (5 samples, 61-px window), M cap 20"},
+            "equal_time": equal_time,
             "frames": n, "ms_per_frame": round(ms / n, 3), "frames_per_s": round(n / (ms / 1e3), 2),
             "render_mrays_per_s": round(segs_per_frame / (split[0] / 8 / 1e3) / 1e6, 1),
             "split_ms_per_frame": {"render": round(split[0] / 8, 3), "temporal": round(split[1] / 8, 3),
                                    "spatial": round(split[2] / 8, 3), "advance": round(split[3] / 8, 3)}}
+
+
+def restir_equal_time(a, dev, s, gs, pipe, col, tg, cams, frame_ms):
+    """Per-frame error of the ReSTIR GI loop against plain path tracing given the same time per frame.
+
+    The orbit loop is replayed from fresh buffers; at each compared frame its output (the spatial
+    pass's image) is kept.  Each kept frame's camera then gets a plain reference of `restir_ref_spp`
+    samples in two independent halves (its own noise, relMSE(A, B) / 4, is subtracted) and a plain
+    render of as many samples as the plain path traces in one ReSTIR frame's time.  relMSE =
+    mean((x - ref)^2 / (ref^2 + 1e-2)) over pixels and colour channels."""
+    import torch
+    import lambent_b200 as lb
+    from lambent_b200 import _abi
+    W, H = s.width, s.height
+    stream = torch.cuda.current_stream()
+    compare = [int(x) for x in a.restir_compare.split(",") if x.strip() and int(x) < len(cams)]
+    fresh = lb.DataBuffers(W, H, 1_500_000, _abi.BUFFER_ALL)
+    kept = {}
+    adv = lb.AdvanceOptions(20)
+    for f in range(len(cams)):
+        pipe.render(gs, fresh, cams[f], tg, f, stream)
+        fresh.temporal_resampling(f, stream)
+        fresh.spatial_resampling(tg, 5, 61, f, stream)
+        fresh.advance_frame(_abi.BUFFER_ALL, adv, stream)
+        if f in compare:
+            kept[f] = col[..., :3].double().clone()
+    del fresh
+    plain_bufs = lb.DataBuffers(W, H, 1, 0)
+
+    def plain_pipe(spp):
+        return lb.RayTracer(lb.path_tracing.Medium).create_pipeline(*s.layout_counts(), lb.PathTracerOpts(
+            samples=spp, restir_temporal=_abi.RESTIR_DISABLED, max_depth=8, guide_mode=_abi.GUIDE_NONE))
+
+    # plain time per sample at this resolution (after a warm-up call)
+    p16 = plain_pipe(16)
+    p16.render(gs, plain_bufs, cams[0], tg, 1, stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(4):
+        p16.render(gs, plain_bufs, cams[0], tg, 2 + k, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_per_spp = e0.elapsed_time(e1) / 64.0
+    spp_eq = max(1, int(round(frame_ms / ms_per_spp)))
+    p_eq = plain_pipe(spp_eq)
+    chunk = min(1024, max(2, a.restir_ref_spp // 2))
+    p_ref = plain_pipe(chunk)
+    rows = []
+    for f in compare:
+        halves = []
+        for h in range(2):
+            acc = torch.zeros((H, W, 3), dtype=torch.float64, device=dev)
+            reps = max(1, a.restir_ref_spp // (2 * chunk))
+            for k in range(reps):
+                p_ref.render(gs, plain_bufs, cams[f], tg, 5_000_000 + 100_000 * f + (h * reps + k) * chunk, stream)
+                acc += col[..., :3].double()
+            halves.append(acc / reps)
+        ref = (halves[0] + halves[1]) / 2
+        den = ref ** 2 + 1e-2
+        noise = float((((halves[0] - halves[1]) ** 2) / den).mean()) / 4.0
+        p_eq.render(gs, plain_bufs, cams[f], tg, 9_000_000 + f, stream)
+        plain = col[..., :3].double()
+        e_plain = float((((plain - ref) ** 2) / den).mean()) - noise
+        e_restir = float((((kept[f] - ref) ** 2) / den).mean()) - noise
+        rows.append({"frame": f, "restir_relmse": round(e_restir, 6), "plain_relmse": round(e_plain, 6),
+                     "ratio": round(e_restir / e_plain, 4) if e_plain > 0 else None,
+                     "ref_noise_relmse": round(noise, 7)})
+    torch.cuda.synchronize()
+    return {"plain_spp_at_equal_time": spp_eq, "plain_ms_per_spp": round(ms_per_spp, 4),
+            "restir_ms_per_frame": round(frame_ms, 3), "reference_spp": 2 * max(1, a.restir_ref_spp // (2 * chunk)) * chunk,
+            "frames": rows,
+            "note": "relMSE of the ReSTIR GI + Markov output of each frame and of a plain render of spp_at_equal_time "
+                    "samples (the plain path's samples in one ReSTIR frame's time), both against a plain reference of "
+                    "the same camera; ratio < 1 means ReSTIR wins at equal time"}
 
 
 def batched_serving(a, dev):

@@ -62,8 +62,15 @@ enum { LAM_RESTIR_DISABLED = 0, LAM_RESTIR_PER_SAMPLE = 1, LAM_RESTIR_PER_PIXEL 
  *                     Markov chain is valid (src/path_tracing/general.wesl:812-815).
  * LAM_GUIDE_MARKOV  - the reference's vMF Markov-chain mixture (general.wesl:764-866).
  * LAM_GUIDE_LEARNED - cosine BSDF sampler combined with the learned lobe mixture by
- *                     one-sample MIS (no counterpart in the reference; see lam_guide). */
-enum { LAM_GUIDE_NONE = 0, LAM_GUIDE_MARKOV = 1, LAM_GUIDE_LEARNED = 2 };
+ *                     one-sample MIS (no counterpart in the reference; see lam_guide).
+ * LAM_GUIDE_PDF_AT_SAMPLE - modifier bit for LAM_GUIDE_MARKOV, no counterpart in the reference.
+ *                     The reference weights a guided sample by 0.2 * cos(w_c)/pi + 0.8 * vMF(w),
+ *                     where w_c is the cosine branch's own draw (general.wesl:793, 840), also when
+ *                     the vMF branch chose w; the estimate is then biased (about +4% on the Cornell
+ *                     box).  With this bit the cosine term is evaluated at w, which makes the
+ *                     mixture pdf the density w was drawn from and the estimator unbiased.  Without
+ *                     it LAM_GUIDE_MARKOV renders what the reference renders. */
+enum { LAM_GUIDE_NONE = 0, LAM_GUIDE_MARKOV = 1, LAM_GUIDE_LEARNED = 2, LAM_GUIDE_PDF_AT_SAMPLE = 4 };
 
 /* BufferType bitflags, src/data_buffer/mod.rs:18-27 */
 enum {
@@ -572,8 +579,15 @@ int lam_guide_loss_grad(lam_guide* guide, const lam_guide_record* records, uint3
 /* steps Adam steps on minibatches of options.batch records drawn from the n device records. */
 int lam_guide_train(lam_guide* guide, const lam_guide_record* records, uint32_t n, uint32_t steps,
                     const float box[6], void* stream);
-/* Number of Adam steps taken and samples per pixel trained so far. */
+/* Number of Adam steps taken and samples per pixel trained so far.  Also reports, once, a
+ * tensor-core completion wait of the guide's kernels that gave up: LAM_ERR_DEVICE_TIMEOUT. */
 int lam_guide_progress(const lam_guide* guide, uint64_t* steps, uint32_t* trained_spp);
+/* Bounded device waits: the polls of an mbarrier that the guide's tensor-core kernels
+ * (lam_guide_eval, lam_guide_loss_grad, lam_guide_train) make before a wait gives up (default 2^20).
+ * A CTA whose wait gives up lets its MMAs in flight finish, frees its tensor memory, records the
+ * timeout and returns; its outputs are then undefined.  0 makes every wait give up at once, which
+ * exercises that path without a stalled device. */
+int lam_guide_set_wait_limit(lam_guide* guide, uint32_t tries);
 /* Attaches the guide used by lam_render when guide_mode is LAM_GUIDE_LEARNED (NULL detaches). */
 int lam_pipeline_set_guide(lam_pipeline* pipeline, lam_guide* guide);
 /* World-space bounds of the scene's geometry: lo xyz, hi xyz. */

@@ -23,12 +23,14 @@ ERR_TEXTURE = -7
 ERR_COMPILE = -8
 ERR_LAYOUT_MISMATCH = -9
 ERR_UNSUPPORTED = -10
+ERR_DEVICE_TIMEOUT = -11
 
 DIFFUSE, METALLIC, TRANSPARENT, SKY = 0, 1, 2, 0xFF
 QUALITY_LOW, QUALITY_MEDIUM, QUALITY_HIGH = 0, 1, 2
 DEBUG_FRONT_FACE, DEBUG_REFLECTANCE, DEBUG_TANGENT = 16, 17, 18
 RESTIR_DISABLED, RESTIR_PER_SAMPLE, RESTIR_PER_PIXEL = 0, 1, 2
 GUIDE_NONE, GUIDE_MARKOV, GUIDE_LEARNED = 0, 1, 2
+GUIDE_PDF_AT_SAMPLE = 4  # modifier of GUIDE_MARKOV: mixture pdf with its cosine term at the chosen direction
 BUFFER_MARKOV_CHAIN_SCREEN_SPACE, BUFFER_SPATIAL_RESAMPLING, BUFFER_MARKOV_CHAIN_WORLD_SPACE = 1, 2, 4
 BUFFER_ALL = 7
 USAGE_COPY_DST, USAGE_UNIFORM, USAGE_STORAGE = 0x8, 0x40, 0x80

@@ -100,6 +100,7 @@ def lib():
     _sig(L, "lam_guide_loss_grad", i, vp, vp, u32, f32p, vp, vp, vp)
     _sig(L, "lam_guide_train", i, vp, vp, u32, u32, f32p, vp)
     _sig(L, "lam_guide_progress", i, vp, P(C.c_uint64), u32p)
+    _sig(L, "lam_guide_set_wait_limit", i, vp, u32)
     _sig(L, "lam_pipeline_set_guide", i, vp, vp)
     _sig(L, "lam_scene_bounds", i, vp, f32p)
     _sig(L, "lam_pipeline_trace_rays", i, vp, vp, vp, u32, u32, vp, vp)
@@ -287,6 +288,9 @@ class GuideMode:
     NONE = _abi.GUIDE_NONE
     MARKOV = _abi.GUIDE_MARKOV
     LEARNED = _abi.GUIDE_LEARNED
+    # the Markov-chain mixture weighted by the density its direction was drawn from (unbiased); MARKOV
+    # alone keeps the reference's weighting, whose cosine term is evaluated at the cosine branch's draw
+    MARKOV_UNBIASED = _abi.GUIDE_MARKOV | _abi.GUIDE_PDF_AT_SAMPLE
 
 
 DEFAULT_NUM_SAMPLES = 4
@@ -633,6 +637,18 @@ def _fbox(box):
     return (C.c_float * 6)(*[float(v) for v in box])
 
 
+def _check_f32(t, name, shape, min_rows=0):
+    """A contiguous CUDA float32 tensor of `shape` (None: any extent) with at least min_rows rows: the
+    guide kernels read and write these through raw device pointers."""
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or not t.is_contiguous() or t.dtype != torch.float32:
+        raise ValueError(f"{name} must be a contiguous CUDA float32 tensor")
+    if t.dim() != len(shape) or any(w is not None and d != w for d, w in zip(t.shape, shape)):
+        raise ValueError(f"{name} must have shape {tuple('n' if w is None else w for w in shape)}")
+    if t.shape[0] < min_rows:
+        raise ValueError(f"{name} holds {t.shape[0]} rows, fewer than {min_rows}")
+
+
 class Guide:
     """The learned guiding network: 4 x 64 x 64 parameters, tcgen05 evaluation and training."""
 
@@ -653,18 +669,29 @@ class Guide:
 
     def eval(self, queries, box, out, stream=None):
         """queries: CUDA float32 (n, 9) = pos, normal, wo; out: CUDA float32 (n, 40) head outputs."""
+        _check_f32(queries, "queries", (None, 9))
+        _check_f32(out, "out", (None, _abi.GUIDE_OUTPUTS), min_rows=queries.shape[0])
         check(lib().lam_guide_eval(self._h, C.c_void_p(queries.data_ptr()), queries.shape[0], _fbox(box),
                                    C.c_void_p(out.data_ptr()), _stream_ptr(stream)))
 
     def loss_grad(self, records, box, grad, loss, stream=None):
         """records: CUDA float32 (n, 13); grad: CUDA float32 (16384,); loss: CUDA float32 (1,)."""
+        _check_f32(records, "records", (None, 13))
+        _check_f32(grad, "grad", (_abi.GUIDE_PARAMS,))
+        _check_f32(loss, "loss", (1,))
         check(lib().lam_guide_loss_grad(self._h, C.c_void_p(records.data_ptr()), records.shape[0], _fbox(box),
                                         C.c_void_p(grad.data_ptr()), C.c_void_p(loss.data_ptr()),
                                         _stream_ptr(stream)))
 
     def train(self, records, steps, box, stream=None):
+        _check_f32(records, "records", (None, 13))
         check(lib().lam_guide_train(self._h, C.c_void_p(records.data_ptr()), records.shape[0], steps, _fbox(box),
                                     _stream_ptr(stream)))
+
+    def set_wait_limit(self, tries):
+        """Polls of a tensor-core completion barrier before a wait gives up (lam_guide_set_wait_limit);
+        0 makes every wait give up at once."""
+        check(lib().lam_guide_set_wait_limit(self._h, int(tries)))
 
     def progress(self):
         st, spp = C.c_uint64(), C.c_uint32()

@@ -52,6 +52,7 @@ struct EvalArgs {
     const uint16_t* packed;
     float* out;            // n x 40
     uint32_t* err;
+    uint32_t wait_tries;   // polls of each completion wait before it gives up
 };
 
 __global__ void __launch_bounds__(128) guide_eval_kernel(EvalArgs A) {
@@ -67,7 +68,7 @@ __global__ void __launch_bounds__(128) guide_eval_kernel(EvalArgs A) {
     fence_before();
     __syncthreads();
     fence_after();
-    TileCtx c{*slot, smem_u32(bar), 0u, false};
+    TileCtx c{*slot, smem_u32(bar), 0u, false, A.wait_tries};
     const uint32_t w_addr = smem_u32(W);
     const uint32_t tiles = (A.n + TILE - 1) / TILE;
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
@@ -87,7 +88,7 @@ __global__ void __launch_bounds__(128) guide_eval_kernel(EvalArgs A) {
         if (idx < A.n)
             for (int k = 0; k < OUT; ++k) A.out[(size_t)idx * OUT + k] = raw[k];
     }
-    if (c.failed) mbar_wait(c.bar, c.phase ^ 1u);  // let an MMA still in flight finish before TMEM is freed
+    if (c.failed) mbar_wait(c.bar, c.phase ^ 1u, DRAIN_TRIES);  // let an MMA in flight finish before TMEM is freed
     fence_before();
     c.failed = __syncthreads_or(c.failed ? 1 : 0) != 0;
     if (c.failed && threadIdx.x == 0) atomicOr(A.err, ERR_MMA_TIMEOUT);
@@ -111,6 +112,7 @@ struct GradArgs {
     float* partial;         // gridDim x PARAMS
     float* partial_loss;    // gridDim
     uint32_t* err;
+    uint32_t wait_tries;    // polls of each completion wait before it gives up
 };
 
 __global__ void __launch_bounds__(128, 1) guide_grad_kernel(GradArgs A) {
@@ -136,7 +138,7 @@ __global__ void __launch_bounds__(128, 1) guide_grad_kernel(GradArgs A) {
     fence_before();
     __syncthreads();
     fence_after();
-    TileCtx c{*slot, smem_u32(bar), 0u, false};
+    TileCtx c{*slot, smem_u32(bar), 0u, false, A.wait_tries};
     const uint32_t row = threadIdx.x;
     const uint32_t t_row = c.tmem + ((threadIdx.x & ~31u) << 16);
     const uint32_t w_addr = smem_u32(W), g_addr = smem_u32(G);
@@ -224,7 +226,7 @@ __global__ void __launch_bounds__(128, 1) guide_grad_kernel(GradArgs A) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) loss += __shfl_down_sync(0xFFFFFFFFu, loss, o);
     if ((threadIdx.x & 31u) == 0u) atomicAdd(sloss, loss);
-    if (c.failed) mbar_wait(c.bar, c.phase ^ 1u);  // let an MMA still in flight finish before TMEM is read or freed
+    if (c.failed) mbar_wait(c.bar, c.phase ^ 1u, DRAIN_TRIES);  // an MMA in flight finishes before TMEM is read or freed
     fence_before();
     c.failed = __syncthreads_or(c.failed ? 1 : 0) != 0;
     fence_after();
@@ -374,6 +376,7 @@ int guide_grad_and_update(lam_guide* g, const float* recs, uint32_t stride, uint
     A.partial = g->partial;
     A.partial_loss = g->partial_loss;
     A.err = g->err;
+    A.wait_tries = g->wait_tries;
     net::guide_grad_kernel<<<grid, 128, net::GRAD_SMEM, st>>>(A);
     net::UpdateArgs U;
     U.partial = g->partial;
@@ -414,6 +417,7 @@ int guide_eval_launch(const lam_guide* g, const float* queries, uint32_t n, cons
     A.packed = g->packed;
     A.out = out;
     A.err = g->err;
+    A.wait_tries = g->wait_tries;
     const uint32_t tiles = (n + net::TILE - 1) / net::TILE;
     const uint32_t grid = std::max(1u, std::min<uint32_t>(tiles, (uint32_t)g->sms * 4u));
     net::guide_eval_kernel<<<grid, 128, net::EVAL_SMEM, st>>>(A);
@@ -426,7 +430,12 @@ int guide_check_error(const lam_guide* g) {
     uint32_t h = 0;
     cudaError_t e = cudaMemcpy(&h, g->err, sizeof(h), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_error(e, "lam_guide error flags");
-    if (h & net::ERR_MMA_TIMEOUT) return set_error(LAM_ERR_CUDA, "guide network: tensor-core wait timed out");
+    if (h & net::ERR_MMA_TIMEOUT) {
+        // reported once: the flags start clear again for the next kernels
+        e = cudaMemset(g->err, 0, sizeof(h));
+        if (e != cudaSuccess) return cuda_error(e, "lam_guide error flags");
+        return set_error(LAM_ERR_DEVICE_TIMEOUT, "guide network: a tensor-core completion wait gave up");
+    }
     return LAM_OK;
 }
 
@@ -529,6 +538,12 @@ extern "C" int lam_guide_train(lam_guide* g, const lam_guide_record* records, ui
                                        1.0f / (float)g->opts.batch, box, 1u, nullptr, nullptr, (cudaStream_t)stream);
         if (rc) return rc;
     }
+    return LAM_OK;
+}
+
+extern "C" int lam_guide_set_wait_limit(lam_guide* g, uint32_t tries) {
+    if (!g) return set_error(LAM_ERR_INVALID_ARGUMENT, "null guide");
+    g->wait_tries = tries;
     return LAM_OK;
 }
 

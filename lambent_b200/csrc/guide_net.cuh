@@ -97,9 +97,13 @@ LAM_DEV void mbar_init(uint64_t* bar) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-// Bounded wait for phase `parity` of the barrier; false when the limit ran out.
-LAM_DEV bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (uint32_t it = 0; it < (1u << 20); ++it) {
+// Polls of a completion barrier before a wait gives up (lam_guide_set_wait_limit), and the polls of
+// the wait that, after a give-up, lets the MMAs still in flight finish before TMEM is read or freed.
+constexpr uint32_t WAIT_TRIES = 1u << 20;
+constexpr uint32_t DRAIN_TRIES = 1u << 22;
+// Bounded wait for phase `parity` of the barrier; false when `tries` polls ran out (0: at once).
+LAM_DEV bool mbar_wait(uint32_t bar, uint32_t parity, uint32_t tries = WAIT_TRIES) {
+    for (uint32_t it = 0; it < tries; ++it) {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -354,6 +358,7 @@ struct TileCtx {
     uint32_t bar;    // shared address of the completion mbarrier
     uint32_t phase;
     bool failed;
+    uint32_t tries;  // polls of each completion wait before it gives up
 };
 
 // One MMA round: publishes this thread's shared-memory writes to the tensor core, lets thread 0 issue
@@ -372,7 +377,7 @@ LAM_DEV bool mma_round(TileCtx& c, Issue issue) {
         issue();
         mma_commit(c.bar);
     }
-    if (!mbar_wait(c.bar, c.phase)) c.failed = true;
+    if (!mbar_wait(c.bar, c.phase, c.tries)) c.failed = true;
     c.phase ^= 1u;
     fence_after();
     return true;

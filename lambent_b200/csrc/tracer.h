@@ -89,6 +89,7 @@ struct lam_guide {
     float* records = nullptr;           // render-side training records, record_capacity entries
     uint64_t steps = 0;
     uint32_t trained_spp = 0;
+    uint32_t wait_tries = 1u << 20;     // lam_guide_set_wait_limit
     bool kernels_ready = false;
     std::vector<void*> allocs;
 };

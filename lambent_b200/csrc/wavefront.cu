@@ -681,7 +681,10 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                                            (cand[k].weight_sum / sum_mc);
                             }
                         }
-                        float avg_pdf = (c0 * cos_pdf) + (c1 == 0.0f ? 0.0f : c1 * fmaxf(mix_pdf, 0.0f));
+                        // general.wesl:840 weights by the cosine pdf of the cosine branch's draw even when
+                        // dir is the vMF draw; LAM_GUIDE_PDF_AT_SAMPLE evaluates it at dir (unbiased)
+                        const float cos_term = GUIDE && A.pdf_at_sample ? fmaxf(dot(dir, is.normal) / PI_F, 0.0f) : cos_pdf;
+                        float avg_pdf = (c0 * cos_term) + (c1 == 0.0f ? 0.0f : c1 * fmaxf(mix_pdf, 0.0f));
                         v3 diffuse = Shader<Q, GUIDE>::make_diffuse(is.color, rd, is.normal, is.tangent, is.roughness.x, dir);
                         cached_pdf = avg_pdf;
                         cached_brdf = fmaxf(dot(dir, is.normal) / PI_F, 0.0f);
@@ -970,8 +973,8 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
     }
     if (failed) {
         // let MMAs still in flight finish before TMEM is freed
-        net::mbar_wait(bar_a, phase ^ 1u);
-        net::mbar_wait(bar_b, phase ^ 1u);
+        net::mbar_wait(bar_a, phase ^ 1u, net::DRAIN_TRIES);
+        net::mbar_wait(bar_b, phase ^ 1u, net::DRAIN_TRIES);
     }
     net::fence_before();
     failed = __syncthreads_or(failed ? 1 : 0) != 0;
@@ -1394,7 +1397,9 @@ extern "C" int lam_tracer_create_pipeline(const lam_tracer* t, const lam_pipelin
     if (o->samples == 0) return set_error(LAM_ERR_INVALID_ARGUMENT, "samples must be nonzero (NonZeroU32)");
     if (o->max_depth == 0 || o->max_depth > 255) return set_error(LAM_ERR_INVALID_ARGUMENT, "max_depth must be in 1..255");
     if (o->restir_temporal > LAM_RESTIR_PER_PIXEL) return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown ReSTIR mode");
-    if (o->guide_mode > LAM_GUIDE_LEARNED) return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown guide mode");
+    if (o->guide_mode != LAM_GUIDE_NONE && o->guide_mode != LAM_GUIDE_MARKOV && o->guide_mode != LAM_GUIDE_LEARNED &&
+        o->guide_mode != (LAM_GUIDE_MARKOV | LAM_GUIDE_PDF_AT_SAMPLE))
+        return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown guide mode");
     if (t->quality > LAM_QUALITY_HIGH && (t->quality < LAM_DEBUG_FRONT_FACE || t->quality > LAM_DEBUG_TANGENT))
         return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown shader");
     lam_pipeline* p = new lam_pipeline();
@@ -1516,7 +1521,7 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         s->emission_count > pl->layout.emission_count || s->attribute_count > pl->layout.attribute_count)
         return set_error(LAM_ERR_LAYOUT_MISMATCH, "scene bindings exceed the pipeline layout counts");
     if (pl->quality >= LAM_DEBUG_FRONT_FACE) return render_debug(pl, s, cam, tg, (cudaStream_t)stream);
-    const bool guide = pl->opts.guide_mode == LAM_GUIDE_MARKOV;
+    const bool guide = (pl->opts.guide_mode & LAM_GUIDE_MARKOV) != 0u;
     const bool learned = pl->opts.guide_mode == LAM_GUIDE_LEARNED;
     const uint32_t restir = pl->opts.restir_temporal;
     if (learned && !pl->guide) return set_error(LAM_ERR_INVALID_ARGUMENT, "LAM_GUIDE_LEARNED needs lam_pipeline_set_guide");
@@ -1540,6 +1545,7 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
     A.max_depth = pl->opts.max_depth;
     A.restir = restir;
     A.seed_offset = seed_offset;
+    A.pdf_at_sample = (pl->opts.guide_mode & LAM_GUIDE_PDF_AT_SAMPLE) != 0u;
     A.tmin = pl->opts.tmin;
     A.tmax = pl->opts.tmax;
     A.ray_o = w->ray_o;

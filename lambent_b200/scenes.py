@@ -193,6 +193,70 @@ def occluded_cornell(width=256, height=256, packer=None):
     return cornell_box(width, height, light_size=0.2, occluder=True, packer=packer)
 
 
+def textured_cornell(width=128, height=128, glass_ior=(1.40, 1.75), seed=7, packer=None):
+    """The Cornell geometry with every shading input non-uniform, so that the material decode of
+    ray_hit (general.wesl:1086-1134) and the IOR pick of the quality hooks are exercised:
+
+      * value-noise diffuse layers of different, non-square sizes; UVs per material that reach past
+        [0, 1] (clamp-to-edge addressing); a recolour texture of random texels;
+      * a noise emission texture on the ceiling light (emissive scale 15) and a wall that emits its
+        own diffuse colour (diffuse scale 0.4);
+      * noise attribute textures: the metal box's roughness and coat roughness vary over its faces,
+        and the glass box is rough;
+      * glass with a wide IOR range (per-path pick in Medium, dispersion in High) and a back wall
+        that is diffuse with an IOR range (the Fresnel choice of general.wesl:735-751 at a diffuse
+        vertex);
+      * a noise cube-map sky behind the open front of the box.
+    """
+    rng = np.random.default_rng(seed)
+    s = cornell_box(width, height, packer=packer)
+    s.name = "textured_cornell"
+    back = s.instances[0]["material_indices"].copy()
+    back[4:6] = 6  # the back wall's two triangles (floor, ceiling, back, left, right: two each)
+    s.instances[0]["material_indices"] = back
+
+    def noise(h, w, lo=0.0, hi=1.0, alpha=None):
+        n = value_noise(rng, max(h, w), octaves=3, base=4)[:h, :w]
+        img = (np.clip(lo + (hi - lo) * n, 0.0, 1.0) * 255).astype(np.uint8)
+        if alpha is not None:
+            img[..., 3] = alpha
+        return img
+
+    s.diffuse = [noise(64, 64, 0.3, 0.9, 255), noise(48, 80, 0.1, 0.8, 255), noise(96, 32, 0.1, 0.8, 255),
+                 noise(16, 16, 0.8, 1.0, 255)]
+    s.emission = [noise(32, 32, 0.4, 1.0, 255)]
+    att_metal = noise(64, 64)
+    att_metal[..., 0:2] = (np.clip(0.05 + 0.55 * att_metal[..., 0:2] / 255.0, 0, 1) * 255).astype(np.uint8)
+    att_metal[..., 2:4] = (0.3 * att_metal[..., 2:4]).astype(np.uint8)
+    att_glass = noise(32, 48)
+    att_glass[..., 0:2] = (np.clip(0.02 + 0.25 * att_glass[..., 0:2] / 255.0, 0, 1) * 255).astype(np.uint8)
+    att_glass[..., 2:4] = 0
+    s.attributes = [att_metal, att_glass]
+    s.recolour = (rng.uniform(0.5, 1.0, (8, 8, 4)) * 255).astype(np.uint8)
+    s.recolour[..., 3] = 255
+
+    def uv3():
+        return tuple(tuple(float(x) for x in rng.uniform(-0.2, 1.2, 2)) for _ in range(3))
+
+    pk = _packer(packer)
+    M = lambda d, e, a, es, ior, ty, rec=(0, 0): pk.material(*uv3(), rec, d, e, a, es, ior, ty)
+    s.materials = [
+        M(0, None, None, EmissionScale(0.0, 0.0), None, MaterialType.Diffuse, (1, 2)),
+        M(1, None, None, EmissionScale(0.0, 0.0), None, MaterialType.Diffuse, (5, 3)),
+        M(2, None, None, EmissionScale(0.0, 0.4), None, MaterialType.Diffuse, (7, 7)),
+        M(3, 0, None, EmissionScale(15.0, 0.0), None, MaterialType.Diffuse),
+        M(0, None, 0, EmissionScale(0.0, 0.0), (1.3, 1.6), MaterialType.Metallic, (2, 6)),
+        M(3, None, 1, EmissionScale(0.0, 0.0), glass_ior, MaterialType.Transparent),
+        M(0, None, None, EmissionScale(0.0, 0.0), (1.3, 1.5), MaterialType.Diffuse, (4, 1)),
+    ]
+    S = 32
+    sky = np.zeros((6, S, S, 4), np.uint8)
+    for f in range(6):
+        sky[f] = noise(S, S, 0.05, 0.6 if f != 2 else 1.0, 255)
+    s.sky = sky
+    return s
+
+
 # ---------------------------------------------------------------- icospheres
 def icosphere(subdiv):
     t = (1.0 + 5 ** 0.5) / 2.0

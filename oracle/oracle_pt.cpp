@@ -282,7 +282,12 @@ struct PT {
     uint64_t segments = 0;
     uint64_t pixels = 0;
 
-    PT(const Scene& s, const RenderParams& pr) : sc(s), p(pr), guide(pr.guide != LAM_GUIDE_NONE) {}
+    // pdf_at_sample: LAM_GUIDE_PDF_AT_SAMPLE, the cosine term of the mixture pdf evaluated at the
+    // chosen direction instead of at the cosine branch's draw (general.wesl:793, 840)
+    bool pdf_at_sample;
+    PT(const Scene& s, const RenderParams& pr)
+        : sc(s), p(pr), guide((pr.guide & LAM_GUIDE_MARKOV) != 0u),
+          pdf_at_sample((pr.guide & LAM_GUIDE_PDF_AT_SAMPLE) != 0u) {}
 
     // ----- quality hooks
     vec3 get_normal(vec3 ray_dir, vec3 normal, vec3 tangent, uint32_t seed, vec2 rough) const {
@@ -743,7 +748,10 @@ struct PT {
                         } else {
                             dir = dir_markov;
                         }
-                        float avg_pdf = (conf0 * cosine_pdf) + (conf1 == 0.0f ? 0.0f : conf1 * wmax(all_vmf_pdfs(L, ray.origin, dir), 0.0f));
+                        // general.wesl:840 weights by the cosine pdf of dir_cosine even when dir is the
+                        // vMF draw; LAM_GUIDE_PDF_AT_SAMPLE evaluates it at dir
+                        float cos_term = pdf_at_sample ? wmax(dot(dir, is.normal) / PI, 0.0f) : cosine_pdf;
+                        float avg_pdf = (conf0 * cos_term) + (conf1 == 0.0f ? 0.0f : conf1 * wmax(all_vmf_pdfs(L, ray.origin, dir), 0.0f));
                         vec3 diffuse = make_diffuse(is.color, ray, is.normal, is.tangent, is.roughness.x, dir);
                         cached_pdf = avg_pdf;
                         cached_brdf = wmax(dot(dir, is.normal) / PI, 0.0f);

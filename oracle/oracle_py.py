@@ -117,6 +117,28 @@ class OraclePacker:
         return OracleCamera(c)
 
 
+def flatten_no_vertex_return(vertices, geometry_stride, indices, triangles_per_geometry, material_table):
+    """The reference's no-vertex-return lookup, restated independently of the library: triangle p of
+    geometry g reads index slots geometry_stride * g + 3p + {0, 1, 2}, or uses the slot numbers
+    themselves when the index array has length 1 (get_vertices, src/bindings.wesl:103-110); its
+    material is material_table[p], the primitive index within its geometry, clamped to the table as
+    a bounds-checked GPU load is (general.wesl:1086).
+
+    Returns (triangle-list vertices (3T, 3) f32, per-triangle material indices (T,) u32)."""
+    vertices = np.asarray(vertices, np.float32).reshape(-1, 4)
+    indices = np.asarray(indices, np.uint32).reshape(-1)
+    table = np.asarray(material_table, np.uint32).reshape(-1)
+    tri_v, tri_m = [], []
+    for g, count in enumerate(triangles_per_geometry):
+        for p in range(count):
+            slot = geometry_stride * g + 3 * p
+            for j in range(3):
+                vi = slot + j if indices.size == 1 else int(indices[slot + j])
+                tri_v.append(vertices[vi, :3])
+            tri_m.append(table[min(p, table.size - 1)])
+    return np.asarray(tri_v, np.float32), np.asarray(tri_m, np.uint32)
+
+
 HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("prim", "<u4"), ("inst", "<u4"), ("kind", "<u4")])
 
 

@@ -69,6 +69,43 @@ def test_eval_matches_oracle(cuda):
     assert g.progress() == (0, 0)
 
 
+def test_device_wait_timeout_is_reported_and_recovers(cuda):
+    """Bounded device waits.  With the wait limit at 0, every tensor-core completion wait of the guide's
+    kernels gives up at once: each CTA lets the MMA it issued finish, frees its tensor memory, records
+    the timeout and returns.  lam_guide_progress reports LAM_ERR_DEVICE_TIMEOUT once, and with the
+    default limit back the next evaluation and gradient match the oracle: the context stays usable."""
+    import torch
+    g = _guide()
+    params = og.init_params(13)
+    g.set_params(params)
+    n = 512
+    rec = _records(n, 14)
+    q = torch.tensor(rec[:, :9], device="cuda")
+    r = torch.tensor(rec, device="cuda")
+    out = torch.zeros((n, 40), dtype=torch.float32, device="cuda")
+    grad = torch.zeros(16384, dtype=torch.float32, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    for call in (lambda: g.eval(q, BOX, out), lambda: g.loss_grad(r, BOX, grad, loss)):
+        g.set_wait_limit(0)
+        call()
+        torch.cuda.synchronize()
+        with pytest.raises(lb.LambentError) as e:
+            g.progress()
+        assert e.value.code == _abi.ERR_DEVICE_TIMEOUT
+        assert g.progress() == (0, 0)  # reported once
+    g.set_wait_limit(1 << 20)
+    out.zero_()
+    g.eval(q, BOX, out)
+    g.loss_grad(r, BOX, grad, loss)
+    torch.cuda.synchronize()
+    assert g.progress() == (0, 0)
+    ref, _ = og.forward(params, og.encode(rec[:, 0:3], rec[:, 3:6], rec[:, 6:9], BOX), use_bf16=True)
+    got = out.cpu().numpy().astype(np.float64)
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-2
+    ref_loss, _ = og.loss_and_grad(params, rec.astype(np.float64), BOX, use_bf16=True)
+    assert float(loss.item()) == pytest.approx(ref_loss, rel=2e-3)
+
+
 def test_loss_and_gradient_match_oracle(cuda):
     import torch
     g = _guide()

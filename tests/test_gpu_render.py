@@ -119,26 +119,41 @@ def test_statistical_agreement_independent_seeds(cuda):
     assert abs(gm.mean() - om.mean()) < 0.02 * om.mean() + 1e-3
 
 
+def _render_means(render, n):
+    v = np.array([render(r)[..., :3].mean() for r in range(n)])
+    return v.mean(), v.std(ddof=1) / np.sqrt(n)
+
+
 def test_markov_guiding_matches_oracle_statistically(cuda):
     """Markov-chain guiding on the GPU against the oracle's sequential restatement of it.
 
     The GPU's world-grid updates race (as the reference's atomics do), so guided renders are
-    compared by their means over independent seeds, not pixel by pixel.  The restated algorithm
-    itself reads about 5 % above plain path tracing on this scene (oracle: 0.226 against 0.215 over
-    8 seeds; per-render sd 0.007), so the check against plain is a looser bound."""
+    compared by the means of 48 independent renders each, within 3 standard errors of their
+    difference (about 2% of the mean).  The reference's own weighting of a guided sample biases it
+    above plain path tracing (the cosine term of its mixture pdf is evaluated at the cosine branch's
+    draw, general.wesl:793, 840): GPU and oracle reproduce that, and both read plain path tracing's
+    mean once the term is evaluated at the chosen direction (GuideMode.MARKOV_UNBIASED)."""
     s = scenes.cornell_box(32, 32)
-    n = 8
-    plain = np.stack([gpu_render(s, 64, restir=_abi.RESTIR_DISABLED, seed=r)["color"][..., :3] for r in range(n)])
-    guided = np.stack([gpu_render(s, 64, restir=_abi.RESTIR_DISABLED, guide=_abi.GUIDE_MARKOV, seed=100 + r)["color"][..., :3]
-                       for r in range(n)])
-    assert np.isfinite(guided).all()
+    n = 48
     osc = O.OracleScene(s)
-    o_guided = np.stack([osc.render(s.camera, 32, 32, samples=64, restir=_abi.RESTIR_DISABLED, guide=_abi.GUIDE_MARKOV,
-                                    seed_offset=100 + r)["color"][..., :3] for r in range(n)])
-    pm, gm, om = plain.mean(), guided.mean(), o_guided.mean()
-    # means of 8 renders: standard error ~0.0025 each, so 0.06 of the mean is about 4 standard errors
-    assert abs(gm - om) < 0.06 * pm, (gm, om, pm)
-    assert abs(gm - pm) < 0.12 * pm, (gm, pm)
+
+    def gpu(guide, base):
+        return lambda r: gpu_render(s, 64, restir=_abi.RESTIR_DISABLED, guide=guide, seed=base + r)["color"]
+
+    def oracle(guide, base):
+        return lambda r: osc.render(s.camera, 32, 32, samples=64, restir=_abi.RESTIR_DISABLED, guide=guide,
+                                    seed_offset=base + r)["color"]
+
+    unbiased = _abi.GUIDE_MARKOV | _abi.GUIDE_PDF_AT_SAMPLE
+    pm, ps = _render_means(gpu(_abi.GUIDE_NONE, 0), n)
+    gm, gs = _render_means(gpu(_abi.GUIDE_MARKOV, 100), n)
+    om, os_ = _render_means(oracle(_abi.GUIDE_MARKOV, 100), n)
+    um, us = _render_means(gpu(unbiased, 300), n)
+    oum, ous = _render_means(oracle(unbiased, 300), n)
+    assert abs(gm - om) < 3.0 * np.hypot(gs, os_), (gm, om, gs, os_)
+    assert abs(um - oum) < 3.0 * np.hypot(us, ous), (um, oum, us, ous)
+    assert abs(um - pm) < 3.0 * np.hypot(us, ps), (um, pm, us, ps)
+    assert gm - pm > 3.0 * np.hypot(gs, ps), (gm, pm, gs, ps)  # the reference's bias, reproduced
 
 
 def test_depth_and_layout_errors(cuda):
