@@ -36,7 +36,8 @@ enum {
     LAM_ERR_LAYOUT_MISMATCH = -9,         /* bound resources exceed the pipeline layout counts */
     LAM_ERR_UNSUPPORTED = -10,
     LAM_ERR_DEVICE_TIMEOUT = -11,         /* a bounded device-side wait gave up */
-    LAM_ERR_STACK_OVERFLOW = -12          /* traversal stack overflow recorded by a kernel */
+    LAM_ERR_STACK_OVERFLOW = -12,         /* traversal stack overflow recorded by a kernel */
+    LAM_ERR_CALLBACK = -13                /* a caller-supplied callback returned nonzero */
 };
 
 /* ---------------------------------------------------------------- enums */
@@ -597,6 +598,25 @@ int lam_scene_bounds(const lam_scene* scene, float box[6]);
  * the n rgba32f device images frames[0..n) (host array of device pointers). */
 int lam_average_frames(const float* const* frames, uint32_t n, uint32_t width, uint32_t height,
                        float* out_rgb, void* stream);
+
+/* ---------------------------------------------------------------- denoiser hand-off
+ * OidnState::new / denoise, examples/cornell_box/src/main.rs:797-963: the averaged frame (RGB f32,
+ * width * height * 3 floats, the layout lam_average_frames writes) goes to host memory, a host-side
+ * filter (OIDN's RayTracing filter in the reference) works on it in place, and the result returns to
+ * the device buffer.  A lam_denoiser owns the pinned host staging of one frame size.
+ * lam_denoise_fn gets the colour (filtered in place) and, when lam_denoiser_run was given them, the
+ * first-hit normal and albedo images repacked to RGB f32 (else NULL); it returns 0, or nonzero for an
+ * error (lam_denoiser_run then returns LAM_ERR_CALLBACK and leaves the device frame unchanged).
+ * lam_denoiser_run synchronises `stream` twice: before the filter runs and after the upload. */
+typedef struct lam_denoiser lam_denoiser;
+typedef int (*lam_denoise_fn)(void* user, float* rgb, const float* normal, const float* albedo,
+                              uint32_t width, uint32_t height);
+int lam_denoiser_create(uint32_t width, uint32_t height, lam_denoiser** out);
+/* rgb: device, width * height * 3 f32, filtered in place; normal / albedo: device rgba32f images of the
+ * same size (lam_frame_targets.normal / .albedo) or NULL. */
+int lam_denoiser_run(lam_denoiser* denoiser, float* rgb, const float* normal, const float* albedo,
+                     lam_denoise_fn filter, void* user, void* stream);
+int lam_denoiser_destroy(lam_denoiser* denoiser);
 
 #ifdef __cplusplus
 }

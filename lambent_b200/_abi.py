@@ -14,7 +14,7 @@ STATUS_NAMES = {
     0: "LAM_OK", -1: "LAM_ERR_INVALID_ARGUMENT", -2: "LAM_ERR_OUT_OF_MEMORY", -3: "LAM_ERR_CUDA",
     -4: "LAM_ERR_NOT_BUILT", -5: "LAM_ERR_PROJECTION_UNINVERTIBLE", -6: "LAM_ERR_VIEW_UNINVERTIBLE",
     -7: "LAM_ERR_TEXTURE", -8: "LAM_ERR_COMPILE", -9: "LAM_ERR_LAYOUT_MISMATCH", -10: "LAM_ERR_UNSUPPORTED",
-    -11: "LAM_ERR_DEVICE_TIMEOUT", -12: "LAM_ERR_STACK_OVERFLOW",
+    -11: "LAM_ERR_DEVICE_TIMEOUT", -12: "LAM_ERR_STACK_OVERFLOW", -13: "LAM_ERR_CALLBACK",
 }
 ERR_INVALID_ARGUMENT = -1
 ERR_PROJECTION_UNINVERTIBLE = -5
@@ -24,6 +24,7 @@ ERR_COMPILE = -8
 ERR_LAYOUT_MISMATCH = -9
 ERR_UNSUPPORTED = -10
 ERR_DEVICE_TIMEOUT = -11
+ERR_CALLBACK = -13
 
 DIFFUSE, METALLIC, TRANSPARENT, SKY = 0, 1, 2, 0xFF
 QUALITY_LOW, QUALITY_MEDIUM, QUALITY_HIGH = 0, 1, 2

@@ -101,6 +101,9 @@ def lib():
     _sig(L, "lam_guide_train", i, vp, vp, u32, u32, f32p, vp)
     _sig(L, "lam_guide_progress", i, vp, P(C.c_uint64), u32p)
     _sig(L, "lam_guide_set_wait_limit", i, vp, u32)
+    _sig(L, "lam_denoiser_create", i, u32, u32, P(vp))
+    _sig(L, "lam_denoiser_run", i, vp, vp, vp, vp, DenoiseFn, vp, vp)
+    _sig(L, "lam_denoiser_destroy", i, vp)
     _sig(L, "lam_pipeline_set_guide", i, vp, vp)
     _sig(L, "lam_scene_bounds", i, vp, f32p)
     _sig(L, "lam_pipeline_trace_rays", i, vp, vp, vp, u32, u32, vp, vp)
@@ -617,6 +620,57 @@ def average_frames(frames, out_rgb, stream=None):
     h, w = f0.shape[0], f0.shape[1]
     ptrs = (C.c_void_p * len(frames))(*[f.data_ptr() for f in frames])
     check(lib().lam_average_frames(ptrs, len(frames), w, h, C.c_void_p(out_rgb.data_ptr()), _stream_ptr(stream)))
+
+
+# ---------------------------------------------------------------- denoiser hand-off (examples/cornell_box/src/main.rs:797-963)
+DenoiseFn = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                        C.c_uint32, C.c_uint32)
+
+
+class Denoiser:
+    """OidnState: pinned host staging of one frame size.  run() hands the averaged frame (and the
+    first-hit normal / albedo AOVs) to a host filter and uploads the filtered frame in place."""
+
+    def __init__(self, width, height):
+        h = C.c_void_p()
+        check(lib().lam_denoiser_create(width, height, C.byref(h)))
+        self._h, self.width, self.height = h, width, height
+
+    def run(self, rgb, filter, normal=None, albedo=None, stream=None):
+        """rgb: CUDA float32 tensor of width * height * 3 elements (lam_average_frames' layout), filtered
+        in place.  normal / albedo: CUDA float32 (H, W, 4) AOVs or None.  filter(rgb, normal, albedo)
+        gets numpy views, (H, W, 3) each (None where not given), and writes the result into rgb; an
+        exception in it becomes LambentError(LAM_ERR_CALLBACK)."""
+        import numpy as np
+        import torch
+        W, H = self.width, self.height
+        if not (isinstance(rgb, torch.Tensor) and rgb.is_cuda and rgb.is_contiguous() and rgb.dtype == torch.float32
+                and rgb.numel() == W * H * 3):
+            raise ValueError("rgb must be a contiguous CUDA float32 tensor of width * height * 3 elements")
+        for name, t in (("normal", normal), ("albedo", albedo)):
+            if t is not None and not (isinstance(t, torch.Tensor) and t.is_cuda and t.is_contiguous()
+                                      and t.dtype == torch.float32 and tuple(t.shape) == (H, W, 4)):
+                raise ValueError(f"{name} must be a contiguous CUDA float32 tensor of shape ({H}, {W}, 4)")
+
+        def view(p):
+            return None if not p else np.ctypeslib.as_array(p, shape=(H, W, 3))
+
+        def call(user, c, n, a, w, h):
+            try:
+                filter(view(c), view(n), view(a))
+                return 0
+            except Exception:
+                return 1
+
+        cb = DenoiseFn(call)
+        ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())
+        check(lib().lam_denoiser_run(self._h, C.c_void_p(rgb.data_ptr()), ptr(normal), ptr(albedo), cb, None,
+                                     _stream_ptr(stream)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.lam_denoiser_destroy(self._h)
+            self._h = None
 
 
 # ---------------------------------------------------------------- learned path guiding (no reference counterpart)
