@@ -13,7 +13,12 @@ from lambent_b200 import _abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblambent_oracle.so")
+# The same restatement built with floating-point contraction (a * b + c fused where the compiler
+# chooses): it differs from LIB_PATH only in last bits, which measures how far same-seed renders
+# can drift apart from last-bit arithmetic differences alone.
+FMA_LIB_PATH = os.path.join(HERE, "liblambent_oracle_fma.so")
 _LIB = None
+_FMA_LIB = None
 
 
 class RenderArgs(C.Structure):
@@ -34,13 +39,32 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-def lib():
-    global _LIB
+def fma_available():
+    """The contracted build needs the host's FMA instructions."""
+    try:
+        return " fma " in (" " + open("/proc/cpuinfo").read().replace("\n", " ") + " ")
+    except OSError:
+        return False
+
+
+def lib(contracted=False):
+    """The oracle library; contracted=True: the build with floating-point contraction (FMA_LIB_PATH)."""
+    global _LIB, _FMA_LIB
+    if contracted:
+        if _FMA_LIB is None:
+            if not os.path.exists(FMA_LIB_PATH):
+                subprocess.run(["make", "-s", "-C", HERE, "liblambent_oracle_fma.so"], check=True)
+            _FMA_LIB = _bind(C.CDLL(FMA_LIB_PATH))
+        return _FMA_LIB
     if _LIB is not None:
         return _LIB
     if not os.path.exists(LIB_PATH):
         build()
-    L = C.CDLL(LIB_PATH)
+    _LIB = _bind(C.CDLL(LIB_PATH))
+    return _LIB
+
+
+def _bind(L):
     vp, i, u32 = C.c_void_p, C.c_int, C.c_uint32
     L.oracle_scene_create.argtypes = [C.POINTER(_abi.SceneDesc), C.POINTER(vp)]
     L.oracle_scene_create.restype = i
@@ -79,7 +103,6 @@ def lib():
     fp = C.POINTER(C.c_float)
     L.oracle_wbw.argtypes = [fp, fp, fp, fp, fp, fp, fp, fp, fp, C.POINTER(C.c_int32)]
     L.oracle_wbw.restype = i
-    _LIB = L
     return L
 
 
@@ -143,10 +166,11 @@ HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("prim", "<u4"),
 
 
 class OracleScene:
-    def __init__(self, scene):
+    def __init__(self, scene, contracted=False):
         self.holder = _abi.SceneDescHolder(scene)
+        self._L = lib(contracted)
         h = C.c_void_p()
-        rc = lib().oracle_scene_create(self.holder.ptr(), C.byref(h))
+        rc = self._L.oracle_scene_create(self.holder.ptr(), C.byref(h))
         if rc != 0:
             raise RuntimeError(f"oracle_scene_create failed: {rc}")
         self._h = h
@@ -155,7 +179,7 @@ class OracleScene:
         rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
         hits = np.zeros(rays.shape[0], dtype=HIT_DTYPE)
         threads = threads or os.cpu_count() or 1
-        rc = lib().oracle_trace(self._h, rays.ctypes.data, rays.shape[0], mode, hits.ctypes.data, threads,
+        rc = self._L.oracle_trace(self._h, rays.ctypes.data, rays.shape[0], mode, hits.ctypes.data, threads,
                                 1 if bruteforce else 0)
         if rc != 0:
             raise RuntimeError(f"oracle_trace failed: {rc}")
@@ -188,7 +212,7 @@ class OracleScene:
         a.out_color = out["color"].ctypes.data
         a.out_normal = out["normal"].ctypes.data
         a.out_albedo = out["albedo"].ctypes.data
-        rc = lib().oracle_render(self._h, C.byref(a))
+        rc = self._L.oracle_render(self._h, C.byref(a))
         if rc != 0:
             raise RuntimeError(f"oracle_render failed: {rc}")
         out["segments"] = a.segments_out
@@ -197,8 +221,8 @@ class OracleScene:
         return out
 
     def __del__(self):
-        if getattr(self, "_h", None) and _LIB is not None:
-            _LIB.oracle_scene_destroy(self._h)
+        if getattr(self, "_h", None) and getattr(self, "_L", None) is not None:
+            self._L.oracle_scene_destroy(self._h)
             self._h = None
 
 

@@ -33,6 +33,9 @@ def built_libraries():
     orc = os.path.join(ROOT, "oracle", "liblambent_oracle.so")
     if _stale(orc, os.path.join(ROOT, "oracle"), (".cpp", ".h")):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    fma = os.path.join(ROOT, "oracle", "liblambent_oracle_fma.so")
+    if os.path.exists(fma) and _stale(fma, os.path.join(ROOT, "oracle"), (".cpp", ".h")):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "liblambent_oracle_fma.so"], check=True)
 
 
 @pytest.fixture(scope="session")
