@@ -64,6 +64,11 @@ enum { LAM_RESTIR_DISABLED = 0, LAM_RESTIR_PER_SAMPLE = 1, LAM_RESTIR_PER_PIXEL 
  * LAM_GUIDE_MARKOV  - the reference's vMF Markov-chain mixture (general.wesl:764-866).
  * LAM_GUIDE_LEARNED - cosine BSDF sampler combined with the learned lobe mixture by
  *                     one-sample MIS (no counterpart in the reference; see lam_guide).
+ * LAM_GUIDE_LEARNED | LAM_GUIDE_MARKOV - a three-way one-sample-MIS mixture: with probability 1 - f
+ *                     the Markov sampler's draw (cosine lobe or a chain's vMF lobe, as LAM_GUIDE_MARKOV
+ *                     draws it), with probability f the network's; the sample is weighted by
+ *                     (1 - f) p_markov(w) + f q(w), p_markov being the Markov mixture's pdf with its
+ *                     cosine term at w (unbiased).  ReSTIR must be disabled.
  * LAM_GUIDE_PDF_AT_SAMPLE - modifier bit for LAM_GUIDE_MARKOV, no counterpart in the reference.
  *                     The reference weights a guided sample by 0.2 * cos(w_c)/pi + 0.8 * vMF(w),
  *                     where w_c is the cosine branch's own draw (general.wesl:793, 840), also when

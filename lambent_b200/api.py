@@ -294,6 +294,8 @@ class GuideMode:
     # the Markov-chain mixture weighted by the density its direction was drawn from (unbiased); MARKOV
     # alone keeps the reference's weighting, whose cosine term is evaluated at the cosine branch's draw
     MARKOV_UNBIASED = _abi.GUIDE_MARKOV | _abi.GUIDE_PDF_AT_SAMPLE
+    # cosine + Markov vMF lobes + the network in one one-sample-MIS mixture
+    LEARNED_MARKOV = _abi.GUIDE_LEARNED | _abi.GUIDE_MARKOV
 
 
 DEFAULT_NUM_SAMPLES = 4

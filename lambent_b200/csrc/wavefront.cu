@@ -168,6 +168,9 @@ LAM_DEV float g_lobe(float x, float u, float t1, float t2) {
 }
 
 // ---------------------------------------------------------------- wave buffers
+// lobes of the Markov mixture kept for the learned-guide kernel: one per resampling candidate
+constexpr uint32_t MIX_LOBES = NUM_RESAMPLES;
+
 struct WaveBuffers {
     uint32_t width = 0, height = 0, npix = 0, spp_wave = 0;
     uint64_t paths = 0;
@@ -192,6 +195,8 @@ struct WaveBuffers {
     uint32_t* dq = nullptr;
     float4 *def_n = nullptr, *def_t = nullptr, *def_c = nullptr, *def_o = nullptr, *def_d = nullptr;
     uint32_t* rec_head = nullptr;
+    float4 *def_r = nullptr, *def_lobe = nullptr;  // learned + Markov: the Markov sampler's draw and lobes
+    float* def_lw = nullptr;
     float4 *phit_a = nullptr, *phit_b = nullptr;  // procedural hits (allocated on first use)
     uint32_t* ctr = nullptr;  // [0..1] queue counts, [2..3] work counters, [4] error flags,
                               // [8..11] segment counters, [12] diffuse-queue count, [13] records
@@ -629,7 +634,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 }
                 const bool reflecting = should_reflect || is.ty == TY_METALLIC;
                 if (!reflecting) {
-                    if (LEARN && is.ty == TY_DIFFUSE && depth + 1u < A.max_depth) {
+                    if (LEARN && !GUIDE && is.ty == TY_DIFFUSE && depth + 1u < A.max_depth) {
                         // the guide kernel draws the direction; it uses the seeds of the cosine branch
                         deferred = true;
                         A.def_n[path] = make_float4(is.normal.x, is.normal.y, is.normal.z, is.roughness.x);
@@ -685,13 +690,38 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                         // dir is the vMF draw; LAM_GUIDE_PDF_AT_SAMPLE evaluates it at dir (unbiased)
                         const float cos_term = GUIDE && A.pdf_at_sample ? fmaxf(dot(dir, is.normal) / PI_F, 0.0f) : cos_pdf;
                         float avg_pdf = (c0 * cos_term) + (c1 == 0.0f ? 0.0f : c1 * fmaxf(mix_pdf, 0.0f));
-                        v3 diffuse = Shader<Q, GUIDE>::make_diffuse(is.color, rd, is.normal, is.tangent, is.roughness.x, dir);
-                        cached_pdf = avg_pdf;
-                        cached_brdf = fmaxf(dot(dir, is.normal) / PI_F, 0.0f);
-                        float nf = fabsf(cached_brdf) / fmaxf(avg_pdf, 0.001f);
-                        color = (color * nf) * diffuse;
-                        orc = (orc * nf) * diffuse;
-                        rd = dir;
+                        if (GUIDE && LEARN && depth + 1u < A.max_depth) {
+                            // learned + Markov: the guide kernel mixes this draw with the network's.  It
+                            // needs the Markov mixture pdf at any direction, so the lobes go with the path;
+                            // the pdf of this draw is recomputed from them (the same function the guide
+                            // kernel evaluates), with the cosine term at the drawn direction
+                            deferred = true;
+                            float pref = c0 * fmaxf(dot(dir, is.normal) / PI_F, 0.0f);
+                            float4* lobe = A.def_lobe + (size_t)path * MIX_LOBES;
+                            float* lw = A.def_lw + (size_t)path * MIX_LOBES;
+#pragma unroll 1
+                            for (int k = 0; k < NUM_RESAMPLES; ++k) {
+                                const bool use = c1 != 0.0f && sum_mc > 0.0f && cand[k].weight_sum > 0.0f;
+                                const v3 mean = use ? normalize(light_dir(cand[k], ro)) : splat(0.0f);
+                                const float kappa = use ? get_kappa(cand[k]) : 0.0f;
+                                const float wk = use ? c1 * (cand[k].weight_sum / sum_mc) : 0.0f;
+                                lobe[k] = make_float4(mean.x, mean.y, mean.z, kappa);
+                                lw[k] = wk;
+                                if (use) pref += wk * vmf_pdf(mean, kappa, dir);
+                            }
+                            A.def_n[path] = make_float4(is.normal.x, is.normal.y, is.normal.z, is.roughness.x);
+                            A.def_t[path] = make_float4(is.tangent.x, is.tangent.y, is.tangent.z, __uint_as_float(seed));
+                            A.def_c[path] = make_float4(is.color.x, is.color.y, is.color.z, c0);
+                            A.def_r[path] = make_float4(dir.x, dir.y, dir.z, pref);
+                        } else {
+                            v3 diffuse = Shader<Q, GUIDE>::make_diffuse(is.color, rd, is.normal, is.tangent, is.roughness.x, dir);
+                            cached_pdf = avg_pdf;
+                            cached_brdf = fmaxf(dot(dir, is.normal) / PI_F, 0.0f);
+                            float nf = fabsf(cached_brdf) / fmaxf(avg_pdf, 0.001f);
+                            color = (color * nf) * diffuse;
+                            orc = (orc * nf) * diffuse;
+                            rd = dir;
+                        }
                     } else if (is.ty == TY_TRANSPARENT) {
                         cached_pdf = 1.0f;
                         cached_brdf = 1.0f;
@@ -788,17 +818,63 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
 constexpr uint32_t GUIDE_SMEM = net::LAYERS * net::LAYER_BYTES + 2u * net::X_BYTES + 64u + 128u;
 constexpr uint32_t GUIDE_TMEM_COLS = 128;  // accumulators of tiles A (columns 0..63) and B (64..127)
 
-template <int Q, bool NET>
+// The Markov sampler's mixture pdf at w from the lobes the shade kernel kept for the path:
+// c0 cos/pi + sum_k w_k vMF_k(w), where w_k already includes the vMF branch's probability.
+LAM_DEV float markov_mixture_pdf(const Args& A, uint32_t path, float c0, v3 n, v3 w) {
+    float p = c0 * fmaxf(dot(w, n) / PI_F, 0.0f);
+    const float4* lobe = A.def_lobe + (size_t)path * MIX_LOBES;
+    const float* lw = A.def_lw + (size_t)path * MIX_LOBES;
+#pragma unroll 1
+    for (int k = 0; k < NUM_RESAMPLES; ++k) {
+        const float wk = lw[k];
+        if (wk != 0.0f) {
+            const float4 l = lobe[k];
+            p += wk * vmf_pdf(mk(l.x, l.y, l.z), l.w, w);
+        }
+    }
+    return p;
+}
+
+// MARKOV: the learned + Markov three-way mixture.  The shade kernel drew the Markov sampler's direction
+// (cosine lobe or a candidate's vMF lobe, with the reference's seeds) and kept its lobes; here that draw
+// is taken with probability 1 - f and the network's with probability f, and the sample is weighted by
+// (1 - f) p_markov(w) + f q(w), p_markov being the Markov sampler's whole mixture pdf.
+template <int Q, bool NET, bool MARKOV>
 LAM_DEV void guide_finish(const Args& A, uint32_t path, const net::Lobes* L, bool& out) {
     const float4 o4 = A.def_o[path], d4 = A.def_d[path], dn = A.def_n[path], dt = A.def_t[path], dc = A.def_c[path];
     const float4 th = A.thr[path], ac = A.acc[path];
     const v3 ro = mk(o4.x, o4.y, o4.z), rd = mk(d4.x, d4.y, d4.z), n = mk(dn.x, dn.y, dn.z), t = mk(dt.x, dt.y, dt.z);
     const uint32_t seed0 = __float_as_uint(dt.w);
     v3 color = mk(th.x, th.y, th.z);
-    const v3 dir_cos = cosine_hemisphere(seed0, n, t);
-    v3 dir = dir_cos;
-    float pdf = fmaxf(dot(dir_cos, n) / PI_F, 0.0f);
-    if (NET) {
+    v3 dir;
+    float pdf;
+    if (MARKOV) {
+        const float4 dr = A.def_r[path];
+        dir = mk(dr.x, dr.y, dr.z);
+        pdf = dr.w;
+        if (NET) {
+            const float f = A.guide_frac;
+            uint32_t h = rand_u32(seed0 ^ 0x68E31DA4u);
+            const float u = rand_f32(h);
+            if (u < f) {
+                h = rand_u32(h);
+                const float u0 = rand_f32(h);
+                h = rand_u32(h);
+                const float u1 = rand_f32(h);
+                h = rand_u32(h);
+                const float u2 = rand_f32(h);
+                dir = net::mixture_sample(*L, u0, u1, u2);
+                pdf = markov_mixture_pdf(A, path, dc.w, n, dir);
+                A.flags[path] |= 0x100u;  // not drawn from a chain's vMF lobe (general.wesl:469-472)
+            }
+            pdf = (1.0f - f) * pdf + f * net::mixture_pdf(*L, dir);
+        }
+    } else {
+        const v3 dir_cos = cosine_hemisphere(seed0, n, t);
+        dir = dir_cos;
+        pdf = fmaxf(dot(dir_cos, n) / PI_F, 0.0f);
+    }
+    if (NET && !MARKOV) {
         const float f = A.guide_frac;
         uint32_t h = rand_u32(seed0 ^ 0x68E31DA4u);
         const float u = rand_f32(h);
@@ -818,6 +894,12 @@ LAM_DEV void guide_finish(const Args& A, uint32_t path, const net::Lobes* L, boo
     const float nf = fabsf(cached_brdf) / fmaxf(pdf, 0.001f);
     const v3 color_pre = color;
     color = (color * nf) * diffuse;
+    if (MARKOV) {
+        // the out-radiance colour the Markov chains train on takes the same factor (general.wesl:863)
+        const float4 oc = A.ort[path];
+        const v3 orc = (mk(oc.x, oc.y, oc.z) * nf) * diffuse;
+        A.ort[path] = make_float4(orc.x, orc.y, orc.z, oc.w);
+    }
     A.thr[path] = make_float4(color.x, color.y, color.z, th.w);
     A.brdf[path] = cached_brdf;
     A.acc[path] = make_float4(ac.x, ac.y, ac.z, pdf);
@@ -839,7 +921,7 @@ LAM_DEV void guide_finish(const Args& A, uint32_t path, const net::Lobes* L, boo
     out = true;
 }
 
-template <int Q, bool NET>
+template <int Q, bool NET, bool MARKOV>
 __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
     const uint32_t n = *A.dq_count;
     const uint32_t lane = threadIdx.x & 31u;
@@ -850,7 +932,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
             uint32_t path = 0;
             if (i < n) {
                 path = A.dq[i];
-                guide_finish<Q, false>(A, path, nullptr, go);
+                guide_finish<Q, false, MARKOV>(A, path, nullptr, go);
             }
             const uint32_t mask = __ballot_sync(0xFFFFFFFFu, go);
             uint32_t slot = 0;
@@ -954,7 +1036,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
             if (v) {
                 net::Lobes L;
                 net::lobes_from_raw(raw, L);
-                guide_finish<Q, true>(A, path, &L, go);
+                guide_finish<Q, true, MARKOV>(A, path, &L, go);
             }
             const uint32_t mask = __ballot_sync(0xFFFFFFFFu, go);
             uint32_t slot = 0;
@@ -1097,7 +1179,8 @@ __global__ void shuffle_kernel(Args A) {
 
 // Device bytes of wave state per path: rays of two queues (64), live state of two queues (96), hit
 // (8), two queue entries (8), state by path (44); ReSTIR / Markov / learned-guide extras.
-constexpr uint64_t WAVE_BYTES_PER_PATH = 220, WAVE_BYTES_FULL = 96, WAVE_BYTES_GUIDE = 32, WAVE_BYTES_LEARNED = 88;
+constexpr uint64_t WAVE_BYTES_PER_PATH = 220, WAVE_BYTES_FULL = 96, WAVE_BYTES_GUIDE = 32, WAVE_BYTES_LEARNED = 88,
+                   WAVE_BYTES_THREE_WAY = 16 + 20 * MIX_LOBES;
 
 static int alloc_wave(WaveBuffers* w, uint32_t npix, bool full, bool guide, bool learned) {
     const size_t P = w->paths;
@@ -1147,6 +1230,11 @@ static int alloc_wave(WaveBuffers* w, uint32_t npix, bool full, bool guide, bool
         rc |= walloc(w, &w->def_o, P);
         rc |= walloc(w, &w->def_d, P);
         rc |= walloc(w, &w->rec_head, P);
+        if (guide) {
+            rc |= walloc(w, &w->def_r, P);
+            rc |= walloc(w, &w->def_lobe, P * MIX_LOBES);
+            rc |= walloc(w, &w->def_lw, P * MIX_LOBES);
+        }
     }
     return rc;
 }
@@ -1173,7 +1261,7 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
     size_t free_b = 0, total_b = 0;
     if (spp_wave > 1 && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
         const uint64_t per_path = WAVE_BYTES_PER_PATH + (full ? WAVE_BYTES_FULL : 0) + (guide ? WAVE_BYTES_GUIDE : 0) +
-                                  (learned ? WAVE_BYTES_LEARNED : 0);
+                                  (learned ? WAVE_BYTES_LEARNED : 0) + (guide && learned ? WAVE_BYTES_THREE_WAY : 0);
         const uint64_t fit = (uint64_t)(free_b / 2) / (per_path * std::max(1u, npix));
         if (fit < spp_wave) {
             spp_wave = (uint32_t)std::max<uint64_t>(1, fit);
@@ -1215,14 +1303,19 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
             if (e == cudaSuccess)
                 e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
         };
-        attrs((const void*)guide_sample_kernel<LAM_QUALITY_LOW, true>);
-        attrs((const void*)guide_sample_kernel<LAM_QUALITY_MEDIUM, true>);
-        attrs((const void*)guide_sample_kernel<LAM_QUALITY_HIGH, true>);
+        attrs((const void*)guide_sample_kernel<LAM_QUALITY_LOW, true, false>);
+        attrs((const void*)guide_sample_kernel<LAM_QUALITY_MEDIUM, true, false>);
+        attrs((const void*)guide_sample_kernel<LAM_QUALITY_HIGH, true, false>);
+        attrs((const void*)guide_sample_kernel<LAM_QUALITY_LOW, true, true>);
+        attrs((const void*)guide_sample_kernel<LAM_QUALITY_MEDIUM, true, true>);
+        attrs((const void*)guide_sample_kernel<LAM_QUALITY_HIGH, true, true>);
         // resident CTAs per SM from the kernel's registers and shared memory (the occupancy query
         // under-reports this kernel); at most 4 keep the 128-column TMEM allocations within 512 columns
         cudaFuncAttributes fa{};
         int regs_sm = 0, smem_sm = 0, smem_reserved = 0;
-        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, (const void*)guide_sample_kernel<LAM_QUALITY_MEDIUM, true>);
+        const void* sized = guide ? (const void*)guide_sample_kernel<LAM_QUALITY_MEDIUM, true, true>
+                                  : (const void*)guide_sample_kernel<LAM_QUALITY_MEDIUM, true, false>;
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, sized);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, pl->device);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, pl->device);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_reserved, cudaDevAttrReservedSharedMemoryPerBlock, pl->device);
@@ -1252,14 +1345,20 @@ int ensure_handler(lam_pipeline* pl) {
 }
 
 template <int Q>
-static void launch_guide(bool net, int grid, cudaStream_t st, const Args& A) {
-    if (net) guide_sample_kernel<Q, true><<<grid, WAVE_BLOCK, GUIDE_SMEM, st>>>(A);
-    else guide_sample_kernel<Q, false><<<grid, WAVE_BLOCK, 0, st>>>(A);
+static void launch_guide(bool net, bool markov, int grid, cudaStream_t st, const Args& A) {
+    if (markov) {
+        if (net) guide_sample_kernel<Q, true, true><<<grid, WAVE_BLOCK, GUIDE_SMEM, st>>>(A);
+        else guide_sample_kernel<Q, false, true><<<grid, WAVE_BLOCK, 0, st>>>(A);
+    } else {
+        if (net) guide_sample_kernel<Q, true, false><<<grid, WAVE_BLOCK, GUIDE_SMEM, st>>>(A);
+        else guide_sample_kernel<Q, false, false><<<grid, WAVE_BLOCK, 0, st>>>(A);
+    }
 }
 
 template <int Q>
 static void launch_shade(bool guide, bool learned, dim3 g, dim3 b, cudaStream_t st, const Args& A) {
-    if (guide) shade_kernel<Q, true, false, false><<<g, b, 0, st>>>(A);
+    if (guide && learned) shade_kernel<Q, true, true, false><<<g, b, 0, st>>>(A);
+    else if (guide) shade_kernel<Q, true, false, false><<<g, b, 0, st>>>(A);
     else if (learned) shade_kernel<Q, false, true, false><<<g, b, 0, st>>>(A);
     else shade_kernel<Q, false, false, false><<<g, b, 0, st>>>(A);
 }
@@ -1398,7 +1497,7 @@ extern "C" int lam_tracer_create_pipeline(const lam_tracer* t, const lam_pipelin
     if (o->max_depth == 0 || o->max_depth > 255) return set_error(LAM_ERR_INVALID_ARGUMENT, "max_depth must be in 1..255");
     if (o->restir_temporal > LAM_RESTIR_PER_PIXEL) return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown ReSTIR mode");
     if (o->guide_mode != LAM_GUIDE_NONE && o->guide_mode != LAM_GUIDE_MARKOV && o->guide_mode != LAM_GUIDE_LEARNED &&
-        o->guide_mode != (LAM_GUIDE_MARKOV | LAM_GUIDE_PDF_AT_SAMPLE))
+        o->guide_mode != (LAM_GUIDE_MARKOV | LAM_GUIDE_PDF_AT_SAMPLE) && o->guide_mode != (LAM_GUIDE_MARKOV | LAM_GUIDE_LEARNED))
         return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown guide mode");
     if (t->quality > LAM_QUALITY_HIGH && (t->quality < LAM_DEBUG_FRONT_FACE || t->quality > LAM_DEBUG_TANGENT))
         return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown shader");
@@ -1522,7 +1621,7 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         return set_error(LAM_ERR_LAYOUT_MISMATCH, "scene bindings exceed the pipeline layout counts");
     if (pl->quality >= LAM_DEBUG_FRONT_FACE) return render_debug(pl, s, cam, tg, (cudaStream_t)stream);
     const bool guide = (pl->opts.guide_mode & LAM_GUIDE_MARKOV) != 0u;
-    const bool learned = pl->opts.guide_mode == LAM_GUIDE_LEARNED;
+    const bool learned = (pl->opts.guide_mode & LAM_GUIDE_LEARNED) != 0u;
     const uint32_t restir = pl->opts.restir_temporal;
     if (learned && !pl->guide) return set_error(LAM_ERR_INVALID_ARGUMENT, "LAM_GUIDE_LEARNED needs lam_pipeline_set_guide");
     if (learned && restir != LAM_RESTIR_DISABLED)
@@ -1608,6 +1707,9 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         A.def_c = w->def_c;
         A.def_o = w->def_o;
         A.def_d = w->def_d;
+        A.def_r = w->def_r;
+        A.def_lobe = w->def_lobe;
+        A.def_lw = w->def_lw;
         A.rec_cap = gd->opts.record_capacity;
         A.rec_count = w->ctr + 13;
         A.guide_w = gd->packed;
@@ -1717,9 +1819,9 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
             if (gd) {
                 const int gg = use_net ? w->grid_guide : w->grid_shade;
                 switch (pl->quality) {
-                    case LAM_QUALITY_LOW: launch_guide<LAM_QUALITY_LOW>(use_net, gg, st, A); break;
-                    case LAM_QUALITY_HIGH: launch_guide<LAM_QUALITY_HIGH>(use_net, gg, st, A); break;
-                    default: launch_guide<LAM_QUALITY_MEDIUM>(use_net, gg, st, A); break;
+                    case LAM_QUALITY_LOW: launch_guide<LAM_QUALITY_LOW>(use_net, guide, gg, st, A); break;
+                    case LAM_QUALITY_HIGH: launch_guide<LAM_QUALITY_HIGH>(use_net, guide, gg, st, A); break;
+                    default: launch_guide<LAM_QUALITY_MEDIUM>(use_net, guide, gg, st, A); break;
                 }
                 ++launches;
             }

@@ -73,6 +73,11 @@ struct Args {
     uint32_t *dq, *dq_count;
     float4 *def_n, *def_t, *def_c;
     float4 *def_o, *def_d;  // a deferred path's origin and incoming, then outgoing, direction (by path)
+    // learned + Markov guiding (three-way mixture): the Markov sampler's direction and pdf, and its
+    // candidate lobes (mean, kappa) with their mixture weights (times the vMF branch's probability)
+    float4* def_r;
+    float4* def_lobe;        // MIX_LOBES per path
+    float* def_lw;           // MIX_LOBES per path; 0: no lobe
     float* recs;             // training records (GUIDE_RECORD_STRIDE floats), null when not training
     uint32_t rec_cap;
     float rec_prob;          // probability that a deferred vertex is recorded
