@@ -60,7 +60,7 @@ def parse():
     p.add_argument("--guided-only", action="store_true", help="run only the guided-vs-plain measurement")
     p.add_argument("--guided-width", type=int, default=1920)
     p.add_argument("--guided-height", type=int, default=1080)
-    p.add_argument("--guided-ref-spp", type=int, default=16384, help="spp of the plain reference image")
+    p.add_argument("--guided-ref-spp", type=int, default=65536, help="spp of the plain reference image")
     p.add_argument("--guided-depth", type=int, default=8)
     p.add_argument("--guided-frac", type=float, default=0.5)
     p.add_argument("--guided-train-spp", type=int, default=32)
