@@ -500,11 +500,18 @@ def restir_equal_time(a, dev, s, gs, pipe, col, tg, cams, frame_ms):
         plain = col[..., :3].double()
         e_plain = float((((plain - ref) ** 2) / den).mean()) - noise
         e_restir = float((((kept[f] - ref) ** 2) / den).mean()) - noise
+        # relMSE is a mean of squares: a few firefly pixels can dominate it, so the share of pixels whose
+        # squared relative error exceeds 100 (error > 10x the reference) is reported beside it
+        fire_r = float(((((kept[f] - ref) ** 2) / den).max(-1)[0] > 100.0).double().mean())
+        fire_p = float(((((plain - ref) ** 2) / den).max(-1)[0] > 100.0).double().mean())
         rows.append({"frame": f, "restir_relmse": round(e_restir, 6), "plain_relmse": round(e_plain, 6),
                      "ratio": round(e_restir / e_plain, 4) if e_plain > 0 else None,
-                     "ref_noise_relmse": round(noise, 7)})
+                     "ref_noise_relmse": round(noise, 7),
+                     "firefly_pixel_share": {"restir": round(fire_r, 7), "plain": round(fire_p, 7)}})
     torch.cuda.synchronize()
+    ratios = sorted(r["ratio"] for r in rows if r["ratio"] is not None)
     return {"plain_spp_at_equal_time": spp_eq, "plain_ms_per_spp": round(ms_per_spp, 4),
+            "median_ratio": ratios[len(ratios) // 2] if ratios else None,
             "restir_ms_per_frame": round(frame_ms, 3), "reference_spp": 2 * max(1, a.restir_ref_spp // (2 * chunk)) * chunk,
             "frames": rows,
             "note": "relMSE of the ReSTIR GI + Markov output of each frame and of a plain render of spp_at_equal_time "

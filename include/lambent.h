@@ -523,7 +523,8 @@ int lam_batch_render(lam_pipeline* pipeline, const lam_batch_request* requests, 
 /* Milliseconds from the start of the last batch to each request's completion (synchronises). */
 int lam_batch_latencies(lam_pipeline* pipeline, uint32_t n, double* ms);
 /* Autotuner: times the batch (samples divided by `spp_divisor`, at least 1) under candidate wave
- * sizes and launch sizes, coordinate by coordinate, and writes the fastest to *out. */
+ * sizes and launch sizes, coordinate by coordinate, each as a CUDA-graph replay (best of three after
+ * a capturing call), and writes the fastest to *out. */
 int lam_batch_autotune(lam_pipeline* pipeline, const lam_batch_request* requests, uint32_t n,
                        uint32_t spp_divisor, lam_batch_tuning* out, void* stream);
 

@@ -184,7 +184,7 @@ LAM_DEV float qone(uint32_t w, uint32_t k) {
 // bits 24..31 in octant order | imask) and the leaf group (leaf_base, item hits in bits 0..23).
 LAM_DEV void intersect_node(const uint4* __restrict__ np, const TravRay& r, float tmin, float tmax, uint2& ng,
                             uint2& tg) {
-    const uint4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
+    const uint4 n0 = ld_keep(np), n1 = ld_keep(np + 1), n2 = ld_keep(np + 2), n3 = ld_keep(np + 3), n4 = ld_keep(np + 4);
     const float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
     const uint32_t imask = n0.w >> 24;
     const float sx = __uint_as_float((n0.w & 0xFFu) << 23);
@@ -428,7 +428,7 @@ struct Traverser {
 #endif
                 continue;
             }
-            const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+            const float4 a = ld_keep(tp), b = ld_keep(tp + 1), c = ld_keep(tp + 2);
             float t;
             if (!wbw_f32(R, a, b, c, best_t, &t)) continue;
             const uint32_t prim = __float_as_uint(a.w);
@@ -549,7 +549,7 @@ struct Traverser {
                 r.ky = (int)((pm >> 2) & 3u);
                 r.kz = (int)((pm >> 4) & 3u);
                 const float4* tp = ws.tris[owner] + 3u * item;
-                const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                const float4 a = ld_keep(tp), b = ld_keep(tp + 1), c = ld_keep(tp + 2);
                 float t;
                 if (wbw_f32(r, a, b, c, ws.lim[owner], &t) && t > ws.tmin[owner]) {
                     const uint32_t u = __float_as_uint(t);
