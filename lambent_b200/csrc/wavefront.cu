@@ -360,13 +360,55 @@ struct Shader {
 
 // 16 screen-space candidates of the sample (general.wesl:367-385), recomputed from the seed the
 // sample started its fill with.
-LAM_DEV void screen_candidates(const Args& A, uint32_t pixel, uint32_t fill_seed, MC* cand) {
+// Where the 21 resampling candidates of a Markov-guided bounce live while the bounce is shaded.
+// LocalCands: a per-thread array (local memory).  SharedCands (LAM_CAND_SMEM): shared memory, field
+// major with one column per thread (conflict-free), the six words of a chain that resampling and the
+// mixture read (light xyz, mean cosine, weight sum, sample count); 64.5 KB per 128-thread CTA.
+struct LocalCands {
+    MC a[NUM_RESAMPLES];
+    LAM_DEV void put(int k, const MC& m) { a[k] = m; }
+    LAM_DEV MC get(int k) const { return a[k]; }
+    LAM_DEV float weight(int k) const { return a[k].weight_sum; }
+};
+constexpr uint32_t CAND_WORDS = 6;
+constexpr uint32_t CAND_SMEM = CAND_WORDS * NUM_RESAMPLES * WAVE_BLOCK * sizeof(float);
+struct SharedCands {
+    float* b;  // this thread's column
+    LAM_DEV float* at(int k, int f) const { return b + (k * (int)CAND_WORDS + f) * WAVE_BLOCK; }
+    LAM_DEV void put(int k, const MC& m) {
+        *at(k, 0) = m.light.x;
+        *at(k, 1) = m.light.y;
+        *at(k, 2) = m.light.z;
+        *at(k, 3) = m.mean_cosine;
+        *at(k, 4) = m.weight_sum;
+        *at(k, 5) = __uint_as_float(m.num_samples);
+    }
+    LAM_DEV MC get(int k) const {
+        MC m;
+        m.light = mk(*at(k, 0), *at(k, 1), *at(k, 2));
+        m.mean_cosine = *at(k, 3);
+        m.weight_sum = *at(k, 4);
+        m.num_samples = __float_as_uint(*at(k, 5));
+        m.score = 0.0f;
+        return m;
+    }
+    LAM_DEV float weight(int k) const { return *at(k, 4); }
+};
+#ifdef LAM_CAND_SMEM
+using Cands = SharedCands;
+constexpr uint32_t GUIDE_SHADE_SMEM = CAND_SMEM;  // dynamic shared memory of the guided shade kernel
+#else
+using Cands = LocalCands;
+constexpr uint32_t GUIDE_SHADE_SMEM = 0;
+#endif
+
+LAM_DEV void screen_candidates(const Args& A, uint32_t pixel, uint32_t fill_seed, Cands& cand) {
     const uint32_t x = pixel % A.width, y = pixel / A.width;
     const uint32_t gbase = x & ~31u;
     uint32_t s = fill_seed;
     const uint32_t sub = rand_u32(s) % 32u;
     MC sh = (gbase + sub < A.width) ? mc_load(A.tent_snap + (uint64_t)y * A.width + gbase + sub) : mc_zero();
-    for (int i = 0; i < 4; ++i) cand[i] = sh;
+    for (int i = 0; i < 4; ++i) cand.put(i, sh);
 #pragma unroll 1
     for (int i = 4; i < 16; ++i) {
         uint32_t xr = rand_u32(s);
@@ -378,9 +420,9 @@ LAM_DEV void screen_candidates(const Args& A, uint32_t pixel, uint32_t fill_seed
         uint64_t idx = (uint32_t)(nx + ny * A.width);
         if (A.old_chains && A.old_chains_len) {
             idx = idx < A.old_chains_len ? idx : A.old_chains_len - 1;
-            cand[i] = mc_load(A.old_chains + idx);
+            cand.put(i, mc_load(A.old_chains + idx));
         } else {
-            cand[i] = mc_zero();
+            cand.put(i, mc_zero());
         }
     }
 }
@@ -600,7 +642,12 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                     seed += 1u;
                 }
                 // fill_mc_world_space_states + resample_mcmm (general.wesl:389-425)
-                MC cand[NUM_RESAMPLES];
+#ifdef LAM_CAND_SMEM
+                extern __shared__ float cand_smem[];
+                Cands cand{cand_smem + threadIdx.x};
+#else
+                Cands cand;
+#endif
                 MC s = mc_zero();
                 if (GUIDE) {
                     screen_candidates(A, pixel, __float_as_uint(pn.w), cand);
@@ -613,18 +660,21 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                         float j0 = rand_f32_ptr(&seed);
                         float j1 = rand_f32_ptr(&seed);
                         v3 jit = (mk(j0, 0.0f, j1) * 0.15000000596046448f) * jm;
-                        cand[k] = grid_load(G, ro + from_onb_no_tangent(jit, is.normal), is.normal, rd, rc);
+                        cand.put(k, grid_load(G, ro + from_onb_no_tangent(jit, is.normal), is.normal, rd, rc));
                         seed += 1u;
                     }
-                    cand[20] = tentative;
+                    cand.put(20, tentative);
                     sum_mc = 0.0f;
+                    int sel = -1;
 #pragma unroll 1
                     for (int k = 0; k < NUM_RESAMPLES; ++k) {
                         seed = rand_u32(seed);
-                        sum_mc += cand[k].weight_sum;
-                        if (rand_f32(seed) * sum_mc < cand[k].weight_sum) s = cand[k];
+                        const float wk = cand.weight(k);
+                        sum_mc += wk;
+                        if (rand_f32(seed) * sum_mc < wk) sel = k;
                         seed = rand_u32(seed);
                     }
+                    if (sel >= 0) s = cand.get(sel);
                 } else {
                     for (int k = 16; k < 20; ++k) {
                         seed = rand_u32(rand_u32(seed)) + 1u;
@@ -681,9 +731,10 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                         if (GUIDE && c1 != 0.0f && sum_mc > 0.0f) {
 #pragma unroll 1
                             for (int k = 0; k < NUM_RESAMPLES; ++k) {
-                                if (!(cand[k].weight_sum > 0.0f)) continue;
-                                mix_pdf += vmf_pdf(normalize(light_dir(cand[k], ro)), get_kappa(cand[k]), dir) *
-                                           (cand[k].weight_sum / sum_mc);
+                                if (!(cand.weight(k) > 0.0f)) continue;
+                                const MC ck = cand.get(k);
+                                mix_pdf += vmf_pdf(normalize(light_dir(ck, ro)), get_kappa(ck), dir) *
+                                           (ck.weight_sum / sum_mc);
                             }
                         }
                         // general.wesl:840 weights by the cosine pdf of the cosine branch's draw even when
@@ -701,10 +752,11 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                             float* lw = A.def_lw + (size_t)path * MIX_LOBES;
 #pragma unroll 1
                             for (int k = 0; k < NUM_RESAMPLES; ++k) {
-                                const bool use = c1 != 0.0f && sum_mc > 0.0f && cand[k].weight_sum > 0.0f;
-                                const v3 mean = use ? normalize(light_dir(cand[k], ro)) : splat(0.0f);
-                                const float kappa = use ? get_kappa(cand[k]) : 0.0f;
-                                const float wk = use ? c1 * (cand[k].weight_sum / sum_mc) : 0.0f;
+                                const MC ck = cand.get(k);
+                                const bool use = c1 != 0.0f && sum_mc > 0.0f && ck.weight_sum > 0.0f;
+                                const v3 mean = use ? normalize(light_dir(ck, ro)) : splat(0.0f);
+                                const float kappa = use ? get_kappa(ck) : 0.0f;
+                                const float wk = use ? c1 * (ck.weight_sum / sum_mc) : 0.0f;
                                 lobe[k] = make_float4(mean.x, mean.y, mean.z, kappa);
                                 lw[k] = wk;
                                 if (use) pref += wk * vmf_pdf(mean, kappa, dir);
@@ -1296,6 +1348,21 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
     occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_kernel<LAM_QUALITY_MEDIUM, false, false, false>, WAVE_BLOCK, 0);
     w->grid_shade = w->sms * std::max(1, occ);
+    if (guide && GUIDE_SHADE_SMEM > 0) {
+        const void* ks[] = {(const void*)shade_kernel<LAM_QUALITY_LOW, true, false, false>,
+                            (const void*)shade_kernel<LAM_QUALITY_MEDIUM, true, false, false>,
+                            (const void*)shade_kernel<LAM_QUALITY_HIGH, true, false, false>,
+                            (const void*)shade_kernel<LAM_QUALITY_LOW, true, true, false>,
+                            (const void*)shade_kernel<LAM_QUALITY_MEDIUM, true, true, false>,
+                            (const void*)shade_kernel<LAM_QUALITY_HIGH, true, true, false>};
+        for (const void* k : ks) {
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GUIDE_SHADE_SMEM);
+            if (e != cudaSuccess) {
+                free_wave(w);
+                return cuda_error(e, "guided shade kernel attributes");
+            }
+        }
+    }
     if (learned) {
         cudaError_t e = cudaSuccess;
         auto attrs = [&](const void* k) {
@@ -1357,8 +1424,8 @@ static void launch_guide(bool net, bool markov, int grid, cudaStream_t st, const
 
 template <int Q>
 static void launch_shade(bool guide, bool learned, dim3 g, dim3 b, cudaStream_t st, const Args& A) {
-    if (guide && learned) shade_kernel<Q, true, true, false><<<g, b, 0, st>>>(A);
-    else if (guide) shade_kernel<Q, true, false, false><<<g, b, 0, st>>>(A);
+    if (guide && learned) shade_kernel<Q, true, true, false><<<g, b, GUIDE_SHADE_SMEM, st>>>(A);
+    else if (guide) shade_kernel<Q, true, false, false><<<g, b, GUIDE_SHADE_SMEM, st>>>(A);
     else if (learned) shade_kernel<Q, false, true, false><<<g, b, 0, st>>>(A);
     else shade_kernel<Q, false, false, false><<<g, b, 0, st>>>(A);
 }
