@@ -63,7 +63,9 @@ enum { LAM_RESTIR_DISABLED = 0, LAM_RESTIR_PER_SAMPLE = 1, LAM_RESTIR_PER_PIXEL 
  *                     Markov chain is valid (src/path_tracing/general.wesl:812-815).
  * LAM_GUIDE_MARKOV  - the reference's vMF Markov-chain mixture (general.wesl:764-866).
  * LAM_GUIDE_LEARNED - cosine BSDF sampler combined with the learned lobe mixture by
- *                     one-sample MIS (no counterpart in the reference; see lam_guide).
+ *                     one-sample MIS (no counterpart in the reference; see lam_guide); at rough
+ *                     metallic vertices (Medium / High, index ratio 1, both roughnesses >= 0.1) the
+ *                     reference's reflection and the learned lobes, weighted by their mixture pdf.
  * LAM_GUIDE_LEARNED | LAM_GUIDE_MARKOV - a three-way one-sample-MIS mixture: with probability 1 - f
  *                     the Markov sampler's draw (cosine lobe or a chain's vMF lobe, as LAM_GUIDE_MARKOV
  *                     draws it), with probability f the network's; the sample is weighted by

@@ -143,6 +143,44 @@ LAM_DEV v3 sample_vndf_ggx(uint32_t seed, v3 view, float2 rough) {
     if (v3_near_zero(out)) out = mk(0.0f, 1.0f, 0.0f);
     return normalize(out);
 }
+// Density (per solid angle) of the direction the reference's metallic bounce produces
+// (general.wesl:718, 892-897): sample_vndf_ggx is given the incoming ray direction v (pointing into
+// the surface), so its point p is uniform on the cap {y >= -wi.y} of the unit sphere, with wi the
+// stretched, normalised v; u = p + wi lies on the unit sphere through the origin, the microfacet
+// normal is m = normalize(S u) with S = diag(ax, 1, ay), the ray is reflected about m and, when that
+// points below the surface, mirrored about the geometric normal.  Change of variables:
+//   u -> direction:     p(u) = 4 (u . wi) / (2 pi (1 + wi.y))   on the cap's image
+//   m = S u / |S u|:    dw_u / dw_m = 1 / (ax ay |S^-1 m|^3)
+//   w = reflect(v, m):  dw_m / dw   = 1 / (4 |w . m|)
+// and the mirror adds the density of the mirrored direction.  w, v in the local frame (y = normal).
+LAM_DEV float metal_raw_pdf(v3 v, v3 wi, float ax, float ay, v3 w) {
+    v3 h = w - v;
+    const float hl = len(h);
+    if (!(hl > 0.0f)) return 0.0f;
+    h = h * (1.0f / hl);
+    if (h.y < 0.0f) h = -h;
+    const v3 us = mk(h.x / ax, h.y, h.z / ay);
+    const float ul = len(us);
+    const v3 u = us * (1.0f / ul);
+    const float uw = dot(u, wi);
+    if (!(uw > 0.0f)) return 0.0f;
+    const float py = 2.0f * uw * u.y - wi.y;  // the cap point p = 2 (u . wi) u - wi
+    if (py < -wi.y) return 0.0f;
+    const float dens_u = 4.0f * uw / (TAU_F * (1.0f + wi.y));
+    const float dens_m = dens_u / (ax * ay * ul * ul * ul);
+    const float wm = fabsf(dot(w, h));
+    return wm > 0.0f ? dens_m / (4.0f * wm) : 0.0f;
+}
+LAM_DEV float metal_pdf(v3 rd, v3 n, v3 t, float ax, float ay, v3 w_world) {
+    const v3 v = to_onb(rd, n, t), w = to_onb(w_world, n, t);
+    if (!(w.y > 0.0f)) return 0.0f;
+    const v3 wi = normalize(mk(v.x * ax, v.y, v.z * ay));
+    return metal_raw_pdf(v, wi, ax, ay, w) + metal_raw_pdf(v, wi, ax, ay, mk(w.x, -w.y, w.z));
+}
+// Metallic vertices the learned guide is mixed in at: a microfacet (Medium / High) reflection with no
+// Fresnel choice (index ratio 1) and both roughnesses at least this
+constexpr float METAL_GUIDE_MIN_ROUGHNESS = 0.1f;
+
 LAM_DEV float reflectance(float c, float ri) {
     float r0 = (1.0f - ri) / (1.0f + ri);
     float r0s = r0 * r0;
@@ -195,8 +233,9 @@ struct WaveBuffers {
     uint32_t* dq = nullptr;
     float4 *def_n = nullptr, *def_t = nullptr, *def_c = nullptr, *def_o = nullptr, *def_d = nullptr;
     uint32_t* rec_head = nullptr;
-    float4 *def_r = nullptr, *def_lobe = nullptr;  // learned + Markov: the Markov sampler's draw and lobes
+    float4 *def_r = nullptr, *def_lobe = nullptr;  // the Markov sampler's or the metal's draw; Markov lobes
     float* def_lw = nullptr;
+    uint32_t* def_kind = nullptr;                  // DEF_DIFFUSE / DEF_METAL
     float4 *phit_a = nullptr, *phit_b = nullptr;  // procedural hits (allocated on first use)
     uint32_t* ctr = nullptr;  // [0..1] queue counts, [2..3] work counters, [4] error flags,
                               // [8..11] segment counters, [12] diffuse-queue count, [13] records
@@ -687,6 +726,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                     if (LEARN && !GUIDE && is.ty == TY_DIFFUSE && depth + 1u < A.max_depth) {
                         // the guide kernel draws the direction; it uses the seeds of the cosine branch
                         deferred = true;
+                        A.def_kind[path] = DEF_DIFFUSE;
                         A.def_n[path] = make_float4(is.normal.x, is.normal.y, is.normal.z, is.roughness.x);
                         A.def_t[path] = make_float4(is.tangent.x, is.tangent.y, is.tangent.z, __uint_as_float(seed));
                         A.def_c[path] = make_float4(is.color.x, is.color.y, is.color.z, 0.0f);
@@ -747,6 +787,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                             // the pdf of this draw is recomputed from them (the same function the guide
                             // kernel evaluates), with the cosine term at the drawn direction
                             deferred = true;
+                            A.def_kind[path] = DEF_DIFFUSE;
                             float pref = c0 * fmaxf(dot(dir, is.normal) / PI_F, 0.0f);
                             float4* lobe = A.def_lobe + (size_t)path * MIX_LOBES;
                             float* lw = A.def_lw + (size_t)path * MIX_LOBES;
@@ -782,8 +823,21 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 } else {
                     cached_pdf = 1.0f;
                     cached_brdf = 1.0f;
+                    const v3 rd_in = rd;
                     rd = reflect(rd, normal);
                     if (dot(rd, is.normal) < 0.0f) rd = reflect(rd, is.normal);
+                    if (LEARN && Q != LAM_QUALITY_LOW && is.ty == TY_METALLIC && ri == 1.0f &&
+                        is.roughness.x >= METAL_GUIDE_MIN_ROUGHNESS && is.roughness.y >= METAL_GUIDE_MIN_ROUGHNESS &&
+                        depth + 1u < A.max_depth) {
+                        // the guide kernel mixes this reflection with the network's lobes (the path's
+                        // throughput already holds the albedo, the whole weight of this bounce)
+                        deferred = true;
+                        A.def_kind[path] = DEF_METAL;
+                        A.def_n[path] = make_float4(is.normal.x, is.normal.y, is.normal.z, is.roughness.x);
+                        A.def_t[path] = make_float4(is.tangent.x, is.tangent.y, is.tangent.z, __uint_as_float(seed));
+                        A.def_r[path] = make_float4(rd.x, rd.y, rd.z, is.roughness.y);
+                        rd = rd_in;  // the deferred path keeps its incoming direction
+                    }
                 }
                 cont = depth + 1u < A.max_depth;
                 terminated = !cont;
@@ -891,8 +945,49 @@ LAM_DEV float markov_mixture_pdf(const Args& A, uint32_t path, float c0, v3 n, v
 // (cosine lobe or a candidate's vMF lobe, with the reference's seeds) and kept its lobes; here that draw
 // is taken with probability 1 - f and the network's with probability f, and the sample is weighted by
 // (1 - f) p_markov(w) + f q(w), p_markov being the Markov sampler's whole mixture pdf.
+// A deferred rough-metal vertex: the reference's reflection (drawn by the shade kernel) with
+// probability 1 - f, the network's lobes with f, weighted by p_metal(w) / ((1 - f) p_metal(w) + f q(w))
+// (the reference's weight of this bounce is 1 once the albedo is in the throughput, i.e. the BSDF
+// times the cosine equals the albedo times p_metal).  Untrained (NET false) it is the reference's
+// bounce, unchanged.
+template <bool NET, bool MARKOV>
+LAM_DEV void guide_finish_metal(const Args& A, uint32_t path, const net::Lobes* L) {
+    const float4 d4 = A.def_d[path], dn = A.def_n[path], dt = A.def_t[path], dr = A.def_r[path];
+    v3 dir = mk(dr.x, dr.y, dr.z);
+    if (NET) {
+        const float4 th = A.thr[path];
+        const v3 rd = mk(d4.x, d4.y, d4.z), n = mk(dn.x, dn.y, dn.z), t = mk(dt.x, dt.y, dt.z);
+        const uint32_t seed0 = __float_as_uint(dt.w);
+        const float f = A.guide_frac;
+        uint32_t h = rand_u32(seed0 ^ 0x68E31DA4u);
+        if (rand_f32(h) < f) {
+            h = rand_u32(h);
+            const float u0 = rand_f32(h);
+            h = rand_u32(h);
+            const float u1 = rand_f32(h);
+            h = rand_u32(h);
+            const float u2 = rand_f32(h);
+            dir = net::mixture_sample(*L, u0, u1, u2);
+        }
+        const float pm = metal_pdf(rd, n, t, dn.w, dr.w, dir);
+        const float mix = (1.0f - f) * pm + f * net::mixture_pdf(*L, dir);
+        const float wgt = mix > 0.0f ? pm / mix : 0.0f;
+        A.thr[path] = make_float4(th.x * wgt, th.y * wgt, th.z * wgt, th.w);
+        if (MARKOV) {
+            const float4 oc = A.ort[path];
+            A.ort[path] = make_float4(oc.x * wgt, oc.y * wgt, oc.z * wgt, oc.w);
+        }
+    }
+    A.def_d[path] = make_float4(dir.x, dir.y, dir.z, 0.0f);
+}
+
 template <int Q, bool NET, bool MARKOV>
 LAM_DEV void guide_finish(const Args& A, uint32_t path, const net::Lobes* L, bool& out) {
+    if (A.def_kind[path] == DEF_METAL) {
+        guide_finish_metal<NET, MARKOV>(A, path, L);
+        out = true;
+        return;
+    }
     const float4 o4 = A.def_o[path], d4 = A.def_d[path], dn = A.def_n[path], dt = A.def_t[path], dc = A.def_c[path];
     const float4 th = A.thr[path], ac = A.acc[path];
     const v3 ro = mk(o4.x, o4.y, o4.z), rd = mk(d4.x, d4.y, d4.z), n = mk(dn.x, dn.y, dn.z), t = mk(dt.x, dt.y, dt.z);
@@ -1231,8 +1326,8 @@ __global__ void shuffle_kernel(Args A) {
 
 // Device bytes of wave state per path: rays of two queues (64), live state of two queues (96), hit
 // (8), two queue entries (8), state by path (44); ReSTIR / Markov / learned-guide extras.
-constexpr uint64_t WAVE_BYTES_PER_PATH = 220, WAVE_BYTES_FULL = 96, WAVE_BYTES_GUIDE = 32, WAVE_BYTES_LEARNED = 88,
-                   WAVE_BYTES_THREE_WAY = 16 + 20 * MIX_LOBES;
+constexpr uint64_t WAVE_BYTES_PER_PATH = 220, WAVE_BYTES_FULL = 96, WAVE_BYTES_GUIDE = 32, WAVE_BYTES_LEARNED = 108,
+                   WAVE_BYTES_THREE_WAY = 20 * MIX_LOBES;
 
 static int alloc_wave(WaveBuffers* w, uint32_t npix, bool full, bool guide, bool learned) {
     const size_t P = w->paths;
@@ -1282,8 +1377,9 @@ static int alloc_wave(WaveBuffers* w, uint32_t npix, bool full, bool guide, bool
         rc |= walloc(w, &w->def_o, P);
         rc |= walloc(w, &w->def_d, P);
         rc |= walloc(w, &w->rec_head, P);
+        rc |= walloc(w, &w->def_r, P);
+        rc |= walloc(w, &w->def_kind, P);
         if (guide) {
-            rc |= walloc(w, &w->def_r, P);
             rc |= walloc(w, &w->def_lobe, P * MIX_LOBES);
             rc |= walloc(w, &w->def_lw, P * MIX_LOBES);
         }
@@ -1775,6 +1871,7 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         A.def_o = w->def_o;
         A.def_d = w->def_d;
         A.def_r = w->def_r;
+        A.def_kind = w->def_kind;
         A.def_lobe = w->def_lobe;
         A.def_lw = w->def_lw;
         A.rec_cap = gd->opts.record_capacity;

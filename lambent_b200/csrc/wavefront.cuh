@@ -8,6 +8,7 @@
 namespace lam {
 
 constexpr int WAVE_BLOCK = 128;
+enum : uint32_t { DEF_DIFFUSE = 0u, DEF_METAL = 1u };  // kinds of vertices deferred to the learned guide
 constexpr uint32_t NO_REC = 0xFFFFFFFFu;
 
 // ---------------------------------------------------------------- batched renders
@@ -75,7 +76,8 @@ struct Args {
     float4 *def_o, *def_d;  // a deferred path's origin and incoming, then outgoing, direction (by path)
     // learned + Markov guiding (three-way mixture): the Markov sampler's direction and pdf, and its
     // candidate lobes (mean, kappa) with their mixture weights (times the vMF branch's probability)
-    float4* def_r;
+    float4* def_r;           // also a rough-metal vertex's reflection (xyz) and roughness y (w)
+    uint32_t* def_kind;      // what a deferred vertex is: DEF_DIFFUSE or DEF_METAL
     float4* def_lobe;        // MIX_LOBES per path
     float* def_lw;           // MIX_LOBES per path; 0: no lobe
     float* recs;             // training records (GUIDE_RECORD_STRIDE floats), null when not training

@@ -188,3 +188,52 @@ def init_params(seed):
         W[l, :, :63] = rng.uniform(-a, a, size=(WIDTH, 63))
         W[l, :, 63] = rng.uniform(-0.1, 0.1, size=WIDTH)
     return (W * trainable_mask()).reshape(-1)
+
+
+# ---------------------------------------------------------------- the reference's metallic bounce
+def metal_sample(v, ax, ay, u1, u2):
+    """The reference's metallic bounce in the local frame (y = the surface normal facing the ray):
+    sample_vndf_ggx(seed, to_onb(ray.direction)) (general.wesl:718, 1246-1281) -- given the INCOMING
+    direction v -- then reflect(v, m) and, when that points below the surface, a mirror about the
+    normal (:892-897).  v: (3,), u1, u2: (N,) uniforms.  Returns (N, 3) directions."""
+    wi = np.array([v[0] * ax, v[1], v[2] * ay], np.float64)
+    wi /= np.linalg.norm(wi)
+    phi = 2.0 * np.pi * u1
+    y = (1.0 - u2) * (1.0 + wi[1]) - wi[1]
+    st = np.sqrt(np.clip(1.0 - y * y, 0.0, 1.0))
+    c = np.stack([st * np.cos(phi), y, st * np.sin(phi)], 1) + wi
+    m = np.stack([c[:, 0] * ax, c[:, 1], c[:, 2] * ay], 1)
+    m /= np.linalg.norm(m, axis=1, keepdims=True)
+    d = v[None, :] - 2.0 * (m @ v)[:, None] * m
+    d[:, 1] = np.abs(d[:, 1])
+    return d
+
+
+def metal_pdf(v, ax, ay, w):
+    """Density per solid angle of metal_sample's directions, derived independently of the CUDA code:
+    the cap point p is uniform on {y >= -wi.y} (area 2 pi (1 + wi.y)); u = p + wi lies on the unit
+    sphere through the origin, where a direction u has density 4 (u . wi) per unit area's worth of
+    solid angle; m = normalize(S u) (S = diag(ax, 1, ay)) has Jacobian 1 / (ax ay |S^-1 m|^3); the
+    reflection w = reflect(v, m) has Jacobian 1 / (4 |w . m|); the mirror adds the density of the
+    mirrored direction.  w: (N, 3) unit directions; 0 below the surface."""
+    wi = np.array([v[0] * ax, v[1], v[2] * ay], np.float64)
+    wi /= np.linalg.norm(wi)
+
+    def raw(o):
+        h = o - v[None, :]
+        hl = np.linalg.norm(h, axis=1, keepdims=True)
+        h = h / np.maximum(hl, 1e-300)
+        h = np.where(h[:, 1:2] < 0, -h, h)
+        us = h / np.array([ax, 1.0, ay])
+        ul = np.linalg.norm(us, axis=1)
+        u = us / ul[:, None]
+        uw = u @ wi
+        py = 2.0 * uw * u[:, 1] - wi[1]
+        ok = (uw > 0) & (py >= -wi[1])
+        dens = np.where(ok, 4.0 * uw / (2.0 * np.pi * (1.0 + wi[1])) / (ax * ay * ul ** 3), 0.0)
+        wm = np.abs((o * h).sum(1))
+        return np.where(wm > 0, dens / (4.0 * np.maximum(wm, 1e-300)), 0.0)
+
+    w = np.asarray(w, np.float64).reshape(-1, 3)
+    mirrored = w * np.array([1.0, -1.0, 1.0])
+    return np.where(w[:, 1] > 0, raw(w) + raw(mirrored), 0.0)
