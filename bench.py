@@ -28,12 +28,17 @@ sys.path.insert(0, ROOT)
 METRIC = "Mrays/s at 1080p/1.3M tris"
 SEG_BYTES_EXTEND = 48   # ray (o, d, tmax) 28 B read + hit 20 B write per segment
 SEG_BYTES_TOTAL = 280   # extend 48 + shade 232 (compulsory wavefront traffic per segment)
-# DRAM bytes (read + write) per segment of the extend kernel, from one ncu capture of all extend
-# launches of a 960x540, 4-spp render of the same scene (profiles/extend_kernel_icosphere_field_960x540.md);
-# traffic grows with the segments processed, so a full launch's traffic is this times its segments.
-EXTEND_DRAM_BYTES_PER_SEGMENT = 138.0
-# What does bound the traversal kernel, from the same kind of capture (ncu --set full of two extend
-# launches of the 960x540 case; profiles/extend_kernel_icosphere_field_960x540.md): instruction issue.
+# DRAM bytes (read + write) per segment of the extend kernel: ncu's dram__bytes_read.sum +
+# dram__bytes_write.sum over the 12 extend launches of one 960x540, 4-spp step of the same scene
+# (7.20M segments; the full 1080p step is too large for a multi-metric capture), from
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum,lts__t_sector_hit_rate.pct
+#       --clock-control none -k regex:extend_kernel -s 36 -c 12 python bench.py --width 960 --height 540 --spp 4
+#       --steps 1 --warmup 3 --no-cpu-baseline --no-guided --no-batched --no-restir
+# Traffic grows with the segments a launch processes, so a full launch's traffic is this times its segments.
+EXTEND_DRAM_BYTES_PER_SEGMENT = 134.5
+# What does bound the traversal kernel, from an ncu capture of two extend launches of the same
+# 960x540 case (sections SpeedOfLight, ComputeWorkloadAnalysis, MemoryWorkloadAnalysis,
+# WarpStateStats; command beside the figures in the extend-kernel profile summary): instruction issue.
 EXTEND_MEASURED_BOUND = {"kind": "instruction issue (BVH and triangles stay in L2)", "issue_slots_busy": 0.736,
                          "alu_pipe": 0.567, "fma_pipe": 0.251, "dram_throughput": 0.012, "l2_hit_rate": 0.846,
                          "threads_per_instruction": 18.3, "l2_gbs": 3090.0,
@@ -351,7 +356,8 @@ def guided_equal_time(a, dev):
         "config": {"workload": f"occluded-light Cornell box (0.2x0.2 emitter above a plate), {W}x{H}, depth "
                                f"{a.guided_depth}, Medium, ReSTIR off",
                    "plain_spp": 1024, "reference_spp": 2 * max(1, a.guided_ref_spp // 2048) * 1024,
-                   "network": "4 x 64 MLP, BF16 tcgen05, 8 vMF lobes, one-sample MIS with the cosine lobe",
+                   "network": "4 x 64 MLP, BF16 tcgen05, 8 vMF lobes, one-sample MIS with the cosine lobe at diffuse "
+                              "vertices and with the reference's reflection at rough metal vertices",
                    "guide_fraction": a.guided_frac, "train_spp": a.guided_train_spp,
                    "adam_steps": steps},
         "plain": {"time_s": round(T, 5), "relmse": round(e_plain, 6), "mrays_per_s": round(segs_plain / T / 1e6, 1)},

@@ -13,46 +13,32 @@ namespace lam {
 #define LAM_DEV __device__ __forceinline__
 
 // Cache policy of the wavefront's loads.  Scene data that every ray of a render revisits (BVH nodes,
-// triangles, instances) goes through the read-only path with the L2 eviction priority evict_last;
+// triangles, instances) goes through the read-only path with an L2 access policy of evict_last;
 // path state that one kernel reads once by queue position goes through ld.global.cs (evict first),
-// so that the gigabytes of path state streamed per step do not push the scene out of L2.
-#ifdef LAM_L2_HINTS
-// An L2 access policy that marks every line it touches evict_last (pure: identical calls fold).
+// so that the gigabytes of path state streamed per step push less of the scene out of L2 (measured
+// on the bench scene: 141 -> 134.5 DRAM bytes per traversal segment, +0.5% rays/s).
 LAM_DEV uint64_t keep_policy() {
     uint64_t pol;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));  // pure: identical calls fold
     return pol;
 }
-#endif
 LAM_DEV uint4 ld_keep(const uint4* p) {
-#ifdef LAM_L2_HINTS
     uint4 v;
     asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
         : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
         : "l"(p), "l"(keep_policy()));
     return v;
-#else
-    return __ldg(p);
-#endif
 }
 LAM_DEV float4 ld_keep(const float4* p) {
-#ifdef LAM_L2_HINTS
     float4 v;
     asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
         : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
         : "l"(p), "l"(keep_policy()));
     return v;
-#else
-    return __ldg(p);
-#endif
 }
 template <class T>
 LAM_DEV T ld_stream(const T* p) {
-#ifdef LAM_L2_HINTS
     return __ldcs(p);
-#else
-    return __ldg(p);
-#endif
 }
 
 struct v3 {

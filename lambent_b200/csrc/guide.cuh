@@ -137,15 +137,7 @@ LAM_DEV MC read_chain_timeout(const uint32_t* e, uint32_t* timeout) {
     return s;
 }
 
-// The world-grid helpers are called from several sites of the guided shade kernel; LAM_GUIDE_NOINLINE
-// keeps one copy of each instead of one per site (a smaller kernel for the instruction cache).
-#ifdef LAM_GUIDE_NOINLINE
-#define LAM_GUIDE_FN static __device__ __noinline__
-#else
-#define LAM_GUIDE_FN LAM_DEV
-#endif
-
-LAM_GUIDE_FN MC grid_load(const Grid& g, v3 pos, v3 normal, v3 incoming, bool force_old) {
+LAM_DEV MC grid_load(const Grid& g, v3 pos, v3 normal, v3 incoming, bool force_old) {
     IVec l = grid_loc(g, pos);
     uint64_t idx = primary_hash(l, normal, incoming) % g.len;
     uint32_t* e = g.world + idx * W_STRIDE;
@@ -180,7 +172,7 @@ LAM_DEV void grid_store(const Grid& g, v3 pos, v3 normal, v3 incoming, const MC&
     vstore2(e + W_CSCORE, __float_as_uint(st.score), CACHE_TIMEOUT);
 }
 
-LAM_GUIDE_FN v3 grid_radiance(const Grid& g, v3 pos, v3 normal, v3 incoming) {
+LAM_DEV v3 grid_radiance(const Grid& g, v3 pos, v3 normal, v3 incoming) {
     IVec l = grid_loc(g, pos);
     uint64_t idx = primary_hash(l, normal, incoming) % g.len;
     uint32_t* e = g.world + idx * W_STRIDE;
@@ -241,7 +233,7 @@ LAM_DEV void grid_add_radiance(const Grid& g, v3 pos, v3 normal, v3 incoming, v3
 // Either is the state that the members' own updates leave when they run one after another without
 // contention, an outcome the reference's relaxed atomics allow (general.wesl:228-311).  Adjacent
 // pixels, which share cells at the first bounces, then no longer queue on one lock and one line.
-LAM_GUIDE_FN void grid_add_radiance_warp(const Grid& g, v3 pos, v3 normal, v3 incoming, v3 radiance) {
+LAM_DEV void grid_add_radiance_warp(const Grid& g, v3 pos, v3 normal, v3 incoming, v3 radiance) {
     const IVec l = grid_loc(g, pos);
     const uint64_t idx = primary_hash(l, normal, incoming) % g.len;
     const uint32_t sec = secondary_hash(l, normal);
@@ -291,7 +283,7 @@ LAM_GUIDE_FN void grid_add_radiance_warp(const Grid& g, v3 pos, v3 normal, v3 in
     }
 }
 
-LAM_GUIDE_FN void grid_store_warp(const Grid& g, v3 pos, v3 normal, v3 incoming, const MC& st) {
+LAM_DEV void grid_store_warp(const Grid& g, v3 pos, v3 normal, v3 incoming, const MC& st) {
     const IVec l = grid_loc(g, pos);
     const uint64_t idx = primary_hash(l, normal, incoming) % g.len;
     const uint32_t sec = secondary_hash(l, normal);
@@ -330,7 +322,7 @@ LAM_DEV float vmf_pdf(v3 mean, float kappa, v3 dir) {
 }
 
 // update_marcov_state, general.wesl:464-492 (sum_mc: the candidate weight sum of the last resample)
-LAM_GUIDE_FN MC update_chain(v3 x1, v3 x2, float p_hat, uint32_t seed, bool not_vmf, MC state, float confidence,
+LAM_DEV MC update_chain(v3 x1, v3 x2, float p_hat, uint32_t seed, bool not_vmf, MC state, float confidence,
                         float sum_mc) {
     if (not_vmf) state = mc_zero();
     float score = p_hat;
