@@ -144,17 +144,20 @@ LAM_DEV v3 sample_vndf_ggx(uint32_t seed, v3 view, float2 rough) {
     return normalize(out);
 }
 // Density (per solid angle) of the direction the reference's metallic bounce produces
-// (general.wesl:718, 892-897): sample_vndf_ggx is given the incoming ray direction v (pointing into
-// the surface), so its point p is uniform on the cap {y >= -wi.y} of the unit sphere, with wi the
-// stretched, normalised v; u = p + wi lies on the unit sphere through the origin, the microfacet
-// normal is m = normalize(S u) with S = diag(ax, 1, ay), the ray is reflected about m and, when that
-// points below the surface, mirrored about the geometric normal.  Change of variables:
-//   u -> direction:     p(u) = 4 (u . wi) / (2 pi (1 + wi.y))   on the cap's image
+// (general.wesl:718, 892-897).  get_normal hands sample_vndf_ggx V = to_onb(rd, n, t), and to_onb
+// (shared.wesl:39-46) is not the inverse of from_onb: for an orthonormal frame it returns
+// -from_onb(rd), so V is a fixed vector of the frame's coordinates, not rd seen from the surface.
+// The sampler's point p is uniform on the cap {y >= -wi.y} of the unit sphere (wi = the stretched,
+// normalised V); u = p + wi lies on the unit sphere through the origin; the microfacet normal is
+// m = normalize(S u) with S = diag(ax, 1, ay), expressed through from_onb; the true incoming
+// direction R (rd in from_onb's frame) is reflected about m and, when that points below the surface,
+// mirrored about the normal.  Change of variables:
+//   u -> direction:     4 (u . wi) / (2 pi (1 + wi.y))   on the cap's image
 //   m = S u / |S u|:    dw_u / dw_m = 1 / (ax ay |S^-1 m|^3)
-//   w = reflect(v, m):  dw_m / dw   = 1 / (4 |w . m|)
-// and the mirror adds the density of the mirrored direction.  w, v in the local frame (y = normal).
-LAM_DEV float metal_raw_pdf(v3 v, v3 wi, float ax, float ay, v3 w) {
-    v3 h = w - v;
+//   w = reflect(R, m):  dw_m / dw   = 1 / (4 |w . m|)
+// and the mirror adds the density of the mirrored direction.
+LAM_DEV float metal_raw_pdf(v3 R, v3 wi, float ax, float ay, v3 w) {
+    v3 h = w - R;
     const float hl = len(h);
     if (!(hl > 0.0f)) return 0.0f;
     h = h * (1.0f / hl);
@@ -172,10 +175,13 @@ LAM_DEV float metal_raw_pdf(v3 v, v3 wi, float ax, float ay, v3 w) {
     return wm > 0.0f ? dens_m / (4.0f * wm) : 0.0f;
 }
 LAM_DEV float metal_pdf(v3 rd, v3 n, v3 t, float ax, float ay, v3 w_world) {
-    const v3 v = to_onb(rd, n, t), w = to_onb(w_world, n, t);
-    if (!(w.y > 0.0f)) return 0.0f;
-    const v3 wi = normalize(mk(v.x * ax, v.y, v.z * ay));
-    return metal_raw_pdf(v, wi, ax, ay, w) + metal_raw_pdf(v, wi, ax, ay, mk(w.x, -w.y, w.z));
+    const v3 t3 = cross(n, t);  // from_onb's third axis
+    const v3 W = mk(dot(w_world, t), dot(w_world, n), dot(w_world, t3));
+    if (!(W.y > 0.0f)) return 0.0f;
+    const v3 V = to_onb(rd, n, t);
+    const v3 R = mk(dot(rd, t), dot(rd, n), dot(rd, t3));
+    const v3 wi = normalize(mk(V.x * ax, V.y, V.z * ay));
+    return metal_raw_pdf(R, wi, ax, ay, W) + metal_raw_pdf(R, wi, ax, ay, mk(W.x, -W.y, W.z));
 }
 // Metallic vertices the learned guide is mixed in at: a microfacet (Medium / High) reflection with no
 // Fresnel choice (index ratio 1) and both roughnesses at least this

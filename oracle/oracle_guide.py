@@ -191,12 +191,28 @@ def init_params(seed):
 
 
 # ---------------------------------------------------------------- the reference's metallic bounce
-def metal_sample(v, ax, ay, u1, u2):
-    """The reference's metallic bounce in the local frame (y = the surface normal facing the ray):
-    sample_vndf_ggx(seed, to_onb(ray.direction)) (general.wesl:718, 1246-1281) -- given the INCOMING
-    direction v -- then reflect(v, m) and, when that points below the surface, a mirror about the
-    normal (:892-897).  v: (3,), u1, u2: (N,) uniforms.  Returns (N, 3) directions."""
-    wi = np.array([v[0] * ax, v[1], v[2] * ay], np.float64)
+def to_onb_ref(src, up, tangent):
+    """to_onb of shared.wesl:39-46 as written: a combination of the cross-product vectors, which for
+    an orthonormal frame equals -from_onb(src) rather than its inverse."""
+    s = np.asarray(tangent, np.float64)
+    up = np.asarray(up, np.float64)
+    t = np.cross(up, s)
+    return src[0] * np.cross(up, t) + src[1] * np.cross(t, s) + src[2] * np.cross(s, up)
+
+
+def metal_frame(rd, n, tangent):
+    """(V, R, axes): V = what get_normal hands sample_vndf_ggx (general.wesl:718); R = rd in the frame
+    from_onb uses (tangent, normal, normal x tangent); axes = that frame's rows."""
+    rd, n, tg = (np.asarray(x, np.float64) for x in (rd, n, tangent))
+    axes = np.stack([tg, n, np.cross(n, tg)])
+    return to_onb_ref(rd, n, tg), axes @ rd, axes
+
+
+def metal_sample(V, R, ax, ay, u1, u2):
+    """The reference's metallic bounce in from_onb's frame (y = the normal facing the ray):
+    sample_vndf_ggx(seed, V) (general.wesl:1246-1281), reflect(rd, m) and, when that points below
+    the surface, a mirror about the normal (:892-897).  u1, u2: (N,) uniforms; returns (N, 3)."""
+    wi = np.array([V[0] * ax, V[1], V[2] * ay], np.float64)
     wi /= np.linalg.norm(wi)
     phi = 2.0 * np.pi * u1
     y = (1.0 - u2) * (1.0 + wi[1]) - wi[1]
@@ -204,23 +220,23 @@ def metal_sample(v, ax, ay, u1, u2):
     c = np.stack([st * np.cos(phi), y, st * np.sin(phi)], 1) + wi
     m = np.stack([c[:, 0] * ax, c[:, 1], c[:, 2] * ay], 1)
     m /= np.linalg.norm(m, axis=1, keepdims=True)
-    d = v[None, :] - 2.0 * (m @ v)[:, None] * m
+    d = R[None, :] - 2.0 * (m @ R)[:, None] * m
     d[:, 1] = np.abs(d[:, 1])
     return d
 
 
-def metal_pdf(v, ax, ay, w):
+def metal_pdf(V, R, ax, ay, w):
     """Density per solid angle of metal_sample's directions, derived independently of the CUDA code:
     the cap point p is uniform on {y >= -wi.y} (area 2 pi (1 + wi.y)); u = p + wi lies on the unit
     sphere through the origin, where a direction u has density 4 (u . wi) per unit area's worth of
     solid angle; m = normalize(S u) (S = diag(ax, 1, ay)) has Jacobian 1 / (ax ay |S^-1 m|^3); the
-    reflection w = reflect(v, m) has Jacobian 1 / (4 |w . m|); the mirror adds the density of the
-    mirrored direction.  w: (N, 3) unit directions; 0 below the surface."""
-    wi = np.array([v[0] * ax, v[1], v[2] * ay], np.float64)
+    reflection w = reflect(R, m) has Jacobian 1 / (4 |w . m|); the mirror adds the density of the
+    mirrored direction.  w: (N, 3) unit directions in the same frame; 0 below the surface."""
+    wi = np.array([V[0] * ax, V[1], V[2] * ay], np.float64)
     wi /= np.linalg.norm(wi)
 
     def raw(o):
-        h = o - v[None, :]
+        h = o - R[None, :]
         hl = np.linalg.norm(h, axis=1, keepdims=True)
         h = h / np.maximum(hl, 1e-300)
         h = np.where(h[:, 1:2] < 0, -h, h)

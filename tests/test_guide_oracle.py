@@ -91,28 +91,38 @@ def test_bf16_gradient_close_to_exact():
 
 
 def test_metal_density_matches_the_reference_sampler():
-    """The density the learned guide's one-sample MIS uses at rough metallic vertices.  The reference's
-    metallic bounce (restated in numpy) is histogrammed over (cos, phi) bins of a frame centred on its
+    """The density the learned guide's one-sample MIS uses at rough metallic vertices.  For random
+    surface frames and rays, the reference's metallic bounce (restated in numpy, with to_onb as the
+    reference writes it) is histogrammed over (cos, phi) bins of a frame centred on its
     mean direction, out to the widest sample, and each bin's count agrees with the derived density
     integrated over the bin; the density integrates to 1 over the hemisphere (uniform Monte Carlo)."""
     rng = np.random.default_rng(4)
-    for v, ax, ay in (([0.5, -0.6, 0.3], 0.35, 0.2), ([0.05, -0.99, -0.1], 0.3, 0.3), ([-0.8, -0.3, 0.52], 0.6, 0.9)):
-        v = np.asarray(v, np.float64)
-        v /= np.linalg.norm(v)
+    cases = []
+    for k in range(4):
+        n0 = rng.normal(size=3)
+        n0 /= np.linalg.norm(n0)
+        tg = np.cross(n0, rng.normal(size=3))
+        tg /= np.linalg.norm(tg)
+        rd = rng.normal(size=3)
+        rd -= (2.0 * max(rd @ n0, 0.0) + 0.2) * n0  # the normal faces the ray
+        rd /= np.linalg.norm(rd)
+        cases.append((rd, n0, tg, [0.35, 0.3, 0.6, 0.15][k], [0.2, 0.3, 0.9, 0.5][k]))
+    for rd, n0, tg, ax, ay in cases:
+        V, R, _ = og.metal_frame(rd, n0, tg)
         u = rng.random((2, 2_000_000))
         ct, ph = u[0], 2.0 * np.pi * u[1]
         st = np.sqrt(1.0 - ct ** 2)
         uni = np.stack([st * np.cos(ph), ct, st * np.sin(ph)], 1)
-        assert abs(og.metal_pdf(v, ax, ay, uni).mean() * 2.0 * np.pi - 1.0) < 0.03  # a few sigma of this estimate
+        assert abs(og.metal_pdf(V, R, ax, ay, uni).mean() * 2.0 * np.pi - 1.0) < 0.03  # a few sigma of this estimate
         n = 1_000_000
-        d = og.metal_sample(v, ax, ay, rng.random(n), rng.random(n))
+        d = og.metal_sample(V, R, ax, ay, rng.random(n), rng.random(n))
         c = d.mean(0)
         c /= np.linalg.norm(c)
         e1 = np.cross(c, [1.0, 0.0, 0.0] if abs(c[0]) < 0.9 else [0.0, 1.0, 0.0])
         e1 /= np.linalg.norm(e1)
         e2 = np.cross(c, e1)
         cmin = (d @ c).min() - 1e-6
-        nt, npb, sub = 12, 24, 10
+        nt, npb, sub = 12, 24, 24
         H, te, pe = np.histogram2d(d @ c, np.arctan2(d @ e2, d @ e1), bins=[nt, npb], range=[[cmin, 1.0], [-np.pi, np.pi]])
         cs = (np.arange(sub) + 0.5) / sub
         exp = np.zeros_like(H)
@@ -123,8 +133,8 @@ def test_metal_density_matches_the_reference_sampler():
                 CC, PP = np.meshgrid(C, P, indexing="ij")
                 S = np.sqrt(np.clip(1.0 - CC ** 2, 0.0, 1.0))
                 o = (CC[..., None] * c + S[..., None] * (np.cos(PP)[..., None] * e1 + np.sin(PP)[..., None] * e2)).reshape(-1, 3)
-                exp[i, j] = og.metal_pdf(v, ax, ay, o).mean() * (te[i + 1] - te[i]) * (pe[j + 1] - pe[j]) * n
-        assert abs(exp.sum() / n - 1.0) < 0.01, exp.sum() / n  # all of the density lies where the samples do
+                exp[i, j] = og.metal_pdf(V, R, ax, ay, o).mean() * (te[i + 1] - te[i]) * (pe[j + 1] - pe[j]) * n
+        assert abs(exp.sum() / n - 1.0) < 0.02, exp.sum() / n  # all of the density lies where the samples do
         m = exp > 400
         rel = np.abs(H[m] - exp[m]) / exp[m]
         assert H[m].sum() / n > 0.8 and np.median(rel) < 0.03, (H[m].sum() / n, np.median(rel))
