@@ -358,7 +358,7 @@ def guided_equal_time(a, dev):
                                f"{a.guided_depth}, Medium, ReSTIR off",
                    "plain_spp": 1024, "reference_spp": 2 * max(1, a.guided_ref_spp // 2048) * 1024,
                    "network": "4 x 64 MLP, BF16 tcgen05, 8 vMF lobes, one-sample MIS with the cosine lobe at diffuse "
-                              "vertices and with the reference's reflection at rough metal vertices",
+                              "vertices",
                    "guide_fraction": a.guided_frac, "train_spp": a.guided_train_spp,
                    "adam_steps": steps},
         "plain": {"time_s": round(T, 5), "relmse": round(e_plain, 6), "mrays_per_s": round(segs_plain / T / 1e6, 1)},

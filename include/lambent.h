@@ -63,9 +63,10 @@ enum { LAM_RESTIR_DISABLED = 0, LAM_RESTIR_PER_SAMPLE = 1, LAM_RESTIR_PER_PIXEL 
  *                     Markov chain is valid (src/path_tracing/general.wesl:812-815).
  * LAM_GUIDE_MARKOV  - the reference's vMF Markov-chain mixture (general.wesl:764-866).
  * LAM_GUIDE_LEARNED - cosine BSDF sampler combined with the learned lobe mixture by
- *                     one-sample MIS (no counterpart in the reference; see lam_guide); at rough
- *                     metallic vertices (Medium / High, index ratio 1, both roughnesses >= 0.1) the
- *                     reference's reflection and the learned lobes, weighted by their mixture pdf.
+ *                     one-sample MIS (no counterpart in the reference; see lam_guide).
+ * LAM_GUIDE_METAL   - modifier bit for the learned modes: the learned lobes are also mixed in at
+ *                     rough metallic vertices (Medium / High, index ratio 1, both roughnesses >= 0.1)
+ *                     with the reference's reflection, weighted by their mixture pdf (unbiased).
  * LAM_GUIDE_LEARNED | LAM_GUIDE_MARKOV - a three-way one-sample-MIS mixture: with probability 1 - f
  *                     the Markov sampler's draw (cosine lobe or a chain's vMF lobe, as LAM_GUIDE_MARKOV
  *                     draws it), with probability f the network's; the sample is weighted by
@@ -78,7 +79,7 @@ enum { LAM_RESTIR_DISABLED = 0, LAM_RESTIR_PER_SAMPLE = 1, LAM_RESTIR_PER_PIXEL 
  *                     box).  With this bit the cosine term is evaluated at w, which makes the
  *                     mixture pdf the density w was drawn from and the estimator unbiased.  Without
  *                     it LAM_GUIDE_MARKOV renders what the reference renders. */
-enum { LAM_GUIDE_NONE = 0, LAM_GUIDE_MARKOV = 1, LAM_GUIDE_LEARNED = 2, LAM_GUIDE_PDF_AT_SAMPLE = 4 };
+enum { LAM_GUIDE_NONE = 0, LAM_GUIDE_MARKOV = 1, LAM_GUIDE_LEARNED = 2, LAM_GUIDE_PDF_AT_SAMPLE = 4, LAM_GUIDE_METAL = 8 };
 
 /* BufferType bitflags, src/data_buffer/mod.rs:18-27 */
 enum {

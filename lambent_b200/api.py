@@ -296,6 +296,8 @@ class GuideMode:
     MARKOV_UNBIASED = _abi.GUIDE_MARKOV | _abi.GUIDE_PDF_AT_SAMPLE
     # cosine + Markov vMF lobes + the network in one one-sample-MIS mixture
     LEARNED_MARKOV = _abi.GUIDE_LEARNED | _abi.GUIDE_MARKOV
+    # modifier of the learned modes: the learned lobes are mixed in at rough metallic vertices too
+    METAL = _abi.GUIDE_METAL
 
 
 DEFAULT_NUM_SAMPLES = 4

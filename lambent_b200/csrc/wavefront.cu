@@ -817,7 +817,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                     const v3 rd_in = rd;
                     rd = reflect(rd, normal);
                     if (dot(rd, is.normal) < 0.0f) rd = reflect(rd, is.normal);
-                    if (LEARN && Q != LAM_QUALITY_LOW && is.ty == TY_METALLIC && ri == 1.0f &&
+                    if (LEARN && A.guide_metal && Q != LAM_QUALITY_LOW && is.ty == TY_METALLIC && ri == 1.0f &&
                         is.roughness.x >= METAL_GUIDE_MIN_ROUGHNESS && is.roughness.y >= METAL_GUIDE_MIN_ROUGHNESS &&
                         depth + 1u < A.max_depth) {
                         // the guide kernel mixes this reflection with the network's lobes (the path's
@@ -936,6 +936,26 @@ LAM_DEV float markov_mixture_pdf(const Args& A, uint32_t path, float c0, v3 n, v
 // (cosine lobe or a candidate's vMF lobe, with the reference's seeds) and kept its lobes; here that draw
 // is taken with probability 1 - f and the network's with probability f, and the sample is weighted by
 // (1 - f) p_markov(w) + f q(w), p_markov being the Markov sampler's whole mixture pdf.
+// Training record of a deferred vertex: the query, the chosen direction and the throughput and
+// accumulated colour at the vertex (finalize_records turns them into the weight when the path ends).
+// A Bernoulli subset of the vertices (probability rec_prob), so that the record buffer samples every
+// pixel and depth of the wave instead of filling up with the first vertices shaded.
+LAM_DEV void record_vertex(const Args& A, uint32_t path, uint32_t seed0, v3 ro, v3 n, v3 rd, v3 dir, v3 color_pre,
+                           float4 ac) {
+    if (A.recs && rand_f32(rand_u32(seed0 ^ 0x2C1B3C6Du)) < A.rec_prob) {
+        const uint32_t r = atomicAdd(A.rec_count, 1u);
+        if (r < A.rec_cap) {
+            float* R = A.recs + (size_t)r * GUIDE_RECORD_STRIDE;
+            const float v[GUIDE_RECORD_STRIDE] = {ro.x, ro.y, ro.z, n.x, n.y, n.z, -rd.x, -rd.y, -rd.z, dir.x,
+                                                  dir.y, dir.z, 0.0f, color_pre.x, color_pre.y, color_pre.z,
+                                                  ac.x, ac.y, ac.z, __uint_as_float(A.rec_head[path])};
+#pragma unroll
+            for (uint32_t k = 0; k < GUIDE_RECORD_STRIDE; ++k) R[k] = v[k];
+            A.rec_head[path] = r;
+        }
+    }
+}
+
 // A deferred rough-metal vertex: the reference's reflection (drawn by the shade kernel) with
 // probability 1 - f, the network's lobes with f, weighted by p_metal(w) / ((1 - f) p_metal(w) + f q(w))
 // (the reference's weight of this bounce is 1 once the albedo is in the throughput, i.e. the BSDF
@@ -1042,20 +1062,7 @@ LAM_DEV void guide_finish(const Args& A, uint32_t path, const net::Lobes* L, boo
     A.brdf[path] = cached_brdf;
     A.acc[path] = make_float4(ac.x, ac.y, ac.z, pdf);
     A.def_d[path] = make_float4(dir.x, dir.y, dir.z, 0.0f);
-    // a Bernoulli subset of the vertices (probability rec_prob), so that the record buffer samples every
-    // pixel and depth of the wave instead of filling up with the first vertices shaded
-    if (A.recs && rand_f32(rand_u32(seed0 ^ 0x2C1B3C6Du)) < A.rec_prob) {
-        const uint32_t r = atomicAdd(A.rec_count, 1u);
-        if (r < A.rec_cap) {
-            float* R = A.recs + (size_t)r * GUIDE_RECORD_STRIDE;
-            const float v[GUIDE_RECORD_STRIDE] = {ro.x, ro.y, ro.z, n.x, n.y, n.z, -rd.x, -rd.y, -rd.z, dir.x,
-                                                  dir.y, dir.z, 0.0f, color_pre.x, color_pre.y, color_pre.z,
-                                                  ac.x, ac.y, ac.z, __uint_as_float(A.rec_head[path])};
-#pragma unroll
-            for (uint32_t k = 0; k < GUIDE_RECORD_STRIDE; ++k) R[k] = v[k];
-            A.rec_head[path] = r;
-        }
-    }
+    record_vertex(A, path, seed0, ro, n, rd, dir, color_pre, ac);
     out = true;
 }
 
@@ -1650,9 +1657,12 @@ extern "C" int lam_tracer_create_pipeline(const lam_tracer* t, const lam_pipelin
     if (o->samples == 0) return set_error(LAM_ERR_INVALID_ARGUMENT, "samples must be nonzero (NonZeroU32)");
     if (o->max_depth == 0 || o->max_depth > 255) return set_error(LAM_ERR_INVALID_ARGUMENT, "max_depth must be in 1..255");
     if (o->restir_temporal > LAM_RESTIR_PER_PIXEL) return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown ReSTIR mode");
-    if (o->guide_mode != LAM_GUIDE_NONE && o->guide_mode != LAM_GUIDE_MARKOV && o->guide_mode != LAM_GUIDE_LEARNED &&
-        o->guide_mode != (LAM_GUIDE_MARKOV | LAM_GUIDE_PDF_AT_SAMPLE) && o->guide_mode != (LAM_GUIDE_MARKOV | LAM_GUIDE_LEARNED))
-        return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown guide mode");
+    {
+        const uint32_t g = o->guide_mode, learned = g & ~(uint32_t)LAM_GUIDE_METAL;
+        const bool ok = g == LAM_GUIDE_NONE || g == LAM_GUIDE_MARKOV || g == (LAM_GUIDE_MARKOV | LAM_GUIDE_PDF_AT_SAMPLE) ||
+                        ((learned == LAM_GUIDE_LEARNED || learned == (LAM_GUIDE_LEARNED | LAM_GUIDE_MARKOV)));
+        if (!ok) return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown guide mode");
+    }
     if (t->quality > LAM_QUALITY_HIGH && (t->quality < LAM_DEBUG_FRONT_FACE || t->quality > LAM_DEBUG_TANGENT))
         return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown shader");
     lam_pipeline* p = new lam_pipeline();
@@ -1799,6 +1809,7 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
     A.restir = restir;
     A.seed_offset = seed_offset;
     A.pdf_at_sample = (pl->opts.guide_mode & LAM_GUIDE_PDF_AT_SAMPLE) != 0u;
+    A.guide_metal = (pl->opts.guide_mode & LAM_GUIDE_METAL) != 0u;
     A.tmin = pl->opts.tmin;
     A.tmax = pl->opts.tmax;
     A.ray_o = w->ray_o;

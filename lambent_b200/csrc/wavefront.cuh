@@ -36,6 +36,7 @@ struct Args {
     float tmin, tmax;
     uint32_t wave_first, wave_count;
     uint32_t pdf_at_sample;  // LAM_GUIDE_PDF_AT_SAMPLE: Markov mixture pdf with its cosine term at the chosen direction
+    uint32_t guide_metal;    // LAM_GUIDE_METAL: the learned guide is mixed in at rough metallic vertices too
     // wave buffers
     float4 *ray_o, *ray_d;          // rays by position in q_in (the generate kernel's queue is the identity)
     float4 *ray_o_out, *ray_d_out;  // rays by position in q_out, written where a path is appended

@@ -35,6 +35,7 @@ pub const LAM_GUIDE_NONE: c_int = 0;
 pub const LAM_GUIDE_MARKOV: c_int = 1;
 pub const LAM_GUIDE_LEARNED: c_int = 2;
 pub const LAM_GUIDE_PDF_AT_SAMPLE: c_int = 4;
+pub const LAM_GUIDE_METAL: c_int = 8;
 pub const LAM_BUFFER_MARKOV_CHAIN_SCREEN_SPACE: c_int = 1 << 0;
 pub const LAM_BUFFER_SPATIAL_RESAMPLING: c_int = 1 << 1;
 pub const LAM_BUFFER_MARKOV_CHAIN_WORLD_SPACE: c_int = 1 << 2;

@@ -285,7 +285,7 @@ def test_untrained_three_way_mixture_is_the_unbiased_markov_estimator(cuda):
 
 
 def test_guide_at_rough_metal_vertices_is_unbiased(cuda):
-    """Rough metallic vertices mix the learned lobes with the reference's reflection (density derived
+    """With GUIDE_METAL, rough metallic vertices mix the learned lobes with the reference's reflection (density derived
     in oracle_guide.metal_pdf, pinned against the reference's sampler on the CPU).  In a box whose
     walls are rough metal (roughness 0.3) and whose light hides above a plate, the trained guide's
     renders agree with plain path tracing on 16 x 16 blocks within 4.5 sigma; untrained, the renders
@@ -295,11 +295,12 @@ def test_guide_at_rough_metal_vertices_is_unbiased(cuda):
     # walls white (0), red (1), green (2) become rough metal with the 0.3-roughness attribute layer
     s.materials = [lb.Material.new((1.0, 1.0), (0.0, 1.0), (1.0, 0.0), (0, 0), d, None, 0, lb.EmissionScale(0.0, 0.0),
                                    None, lb.MaterialType.Metallic) for d in (0, 1, 2)] + list(m[3:])
+    mode = _abi.GUIDE_LEARNED | _abi.GUIDE_METAL
     plain, _, _ = _render(s, 16)
-    untrained, _, _ = _render(s, 16, _abi.GUIDE_LEARNED, _guide(train_spp=0))
+    untrained, _, _ = _render(s, 16, mode, _guide(train_spp=0))
     assert np.array_equal(plain, untrained)
     g = _guide(train_spp=64, record_capacity=1 << 20, batch=8192, steps_per_wave=200, seed=9)
-    _, gpipe, gs = _render(s, 64, _abi.GUIDE_LEARNED, g, seed=1000)
+    _, gpipe, gs = _render(s, 64, mode, g, seed=1000)
     reps, spp = 8, 64
     guided = [_render(s, spp, seed=2000 + k, pipe=gpipe, gscene=gs)[0] for k in range(reps)]
     ppipe, plain = None, []
