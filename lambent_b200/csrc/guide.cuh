@@ -67,9 +67,17 @@ LAM_DEV void vstore(uint32_t* p, uint32_t v) { *(volatile uint32_t*)p = v; }
 struct Grid {
     uint32_t* world;
     const uint32_t* old_world;
-    uint64_t len;
+    uint64_t len;      // cells (< 2^32: the buffer size is a u32)
+    uint64_t mod_m;    // ~0 / len + 1 (computed on the host)
     v3 camera_loc;
 };
+
+// hash % len without a 64-bit division: Lemire's fast remainder for 32-bit operands (Lemire, Kaser
+// and Kurz, "Faster remainder by direct computation", 2019) with m = floor((2^64 - 1) / len) + 1;
+// exact for every 32-bit hash and 0 < len < 2^32 (len = 1 gives m = 0 and the remainder 0).
+LAM_DEV uint64_t grid_index(const Grid& g, uint32_t hash) {
+    return __umul64hi(g.mod_m * (uint64_t)hash, g.len);
+}
 
 struct IVec { int32_t x, y, z; };
 
@@ -139,7 +147,7 @@ LAM_DEV MC read_chain_timeout(const uint32_t* e, uint32_t* timeout) {
 
 LAM_DEV MC grid_load(const Grid& g, v3 pos, v3 normal, v3 incoming, bool force_old) {
     IVec l = grid_loc(g, pos);
-    uint64_t idx = primary_hash(l, normal, incoming) % g.len;
+    uint64_t idx = grid_index(g, primary_hash(l, normal, incoming));
     uint32_t* e = g.world + idx * W_STRIDE;
     uint32_t sec = secondary_hash(l, normal);
     uint32_t timeout = 0u;
@@ -160,7 +168,7 @@ LAM_DEV MC grid_load(const Grid& g, v3 pos, v3 normal, v3 incoming, bool force_o
 
 LAM_DEV void grid_store(const Grid& g, v3 pos, v3 normal, v3 incoming, const MC& st) {
     IVec l = grid_loc(g, pos);
-    uint64_t idx = primary_hash(l, normal, incoming) % g.len;
+    uint64_t idx = grid_index(g, primary_hash(l, normal, incoming));
     uint32_t* e = g.world + idx * W_STRIDE;
     uint32_t sec = secondary_hash(l, normal);
     if (vload(e + W_SEC) != sec) {
@@ -174,7 +182,7 @@ LAM_DEV void grid_store(const Grid& g, v3 pos, v3 normal, v3 incoming, const MC&
 
 LAM_DEV v3 grid_radiance(const Grid& g, v3 pos, v3 normal, v3 incoming) {
     IVec l = grid_loc(g, pos);
-    uint64_t idx = primary_hash(l, normal, incoming) % g.len;
+    uint64_t idx = grid_index(g, primary_hash(l, normal, incoming));
     uint32_t* e = g.world + idx * W_STRIDE;
     const uint2 sn = vload2(e + W_SEC), l01 = vload2(e + W_LUM);  // (tag, count), (radiance x, y)
     uint32_t num = sn.y;
@@ -197,7 +205,7 @@ LAM_DEV v3 grid_radiance(const Grid& g, v3 pos, v3 normal, v3 incoming) {
 
 LAM_DEV void grid_add_radiance(const Grid& g, v3 pos, v3 normal, v3 incoming, v3 radiance) {
     IVec l = grid_loc(g, pos);
-    uint64_t idx = primary_hash(l, normal, incoming) % g.len;
+    uint64_t idx = grid_index(g, primary_hash(l, normal, incoming));
     uint32_t* e = g.world + idx * W_STRIDE;
     uint32_t sec = secondary_hash(l, normal);
     v3 c = clamp3(radiance, 0.0f, 100.0f);
@@ -235,7 +243,7 @@ LAM_DEV void grid_add_radiance(const Grid& g, v3 pos, v3 normal, v3 incoming, v3
 // pixels, which share cells at the first bounces, then no longer queue on one lock and one line.
 LAM_DEV void grid_add_radiance_warp(const Grid& g, v3 pos, v3 normal, v3 incoming, v3 radiance) {
     const IVec l = grid_loc(g, pos);
-    const uint64_t idx = primary_hash(l, normal, incoming) % g.len;
+    const uint64_t idx = grid_index(g, primary_hash(l, normal, incoming));
     const uint32_t sec = secondary_hash(l, normal);
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned grp = __match_any_sync(__activemask(), (idx << 32) | sec);
@@ -285,7 +293,7 @@ LAM_DEV void grid_add_radiance_warp(const Grid& g, v3 pos, v3 normal, v3 incomin
 
 LAM_DEV void grid_store_warp(const Grid& g, v3 pos, v3 normal, v3 incoming, const MC& st) {
     const IVec l = grid_loc(g, pos);
-    const uint64_t idx = primary_hash(l, normal, incoming) % g.len;
+    const uint64_t idx = grid_index(g, primary_hash(l, normal, incoming));
     const uint32_t sec = secondary_hash(l, normal);
     const unsigned grp = __match_any_sync(__activemask(), (idx << 32) | sec);
     if ((threadIdx.x & 31u) == 31u - __clz(grp)) grid_store(g, pos, normal, incoming, st);
@@ -308,17 +316,21 @@ LAM_DEV float exp_minus_one(float x) {
     return y;
 }
 
-LAM_DEV float x_div_exp_minus_one(float x) {
-    float u = expf(x);
-    if (u == 1.0f) return 1.0f;
-    float y = u - 1.0f;
-    if (fabsf(x) < 1.0f) return logf(u) / y;
-    return x / y;
-}
-
-LAM_DEV float vmf_pdf(v3 mean, float kappa, v3 dir) {
-    float fraction = x_div_exp_minus_one(-2.0f * kappa) / (4.0f * PI_F);
-    return fmaxf(fraction * expf(kappa * (dot(dir, mean) - 1.0f)), 0.0f);
+// vmf_pdf with the fast hardware exponential, logarithm and division.  Their error bounds (CUDA:
+// __expf 2 + 1.17|x| ulp, __logf 2^-21.41 absolute in [0.5, 2] and 3 ulp outside, __fdividef 2 ulp)
+// lie within WGSL's accuracy requirements for exp (3 + 2|x| ulp), log (2^-21 absolute in [0.5, 2],
+// 3 ulp outside) and division (2.5 ulp), which are all the reference's all_vmf_pdfs
+// (general.wesl:984-1023) relies on.  Used for the mixture pdf, evaluated for every candidate of
+// every guided bounce; the vMF draw itself keeps the precise functions.
+LAM_DEV float vmf_pdf_fast(v3 mean, float kappa, v3 dir) {
+    const float x = -2.0f * kappa;
+    const float u = __expf(x);
+    float frac = 1.0f;
+    if (u != 1.0f) {
+        const float y = u - 1.0f;
+        frac = fabsf(x) < 1.0f ? __fdividef(__logf(u), y) : __fdividef(x, y);
+    }
+    return fmaxf(frac * (1.0f / (4.0f * PI_F)) * __expf(kappa * (dot(dir, mean) - 1.0f)), 0.0f);
 }
 
 // update_marcov_state, general.wesl:464-492 (sum_mc: the candidate weight sum of the last resample)

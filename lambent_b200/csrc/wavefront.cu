@@ -409,7 +409,9 @@ struct Shader {
 // shaded: field major with one column per thread (conflict-free), the six words of a chain that
 // resampling and the mixture read (light xyz, mean cosine, weight sum, sample count); 64.5 KB per
 // 128-thread CTA.  As a per-thread array they lived in local memory (616 bytes of stack per thread,
-// spilling out of L1 at 12 warps per SM); here the ReSTIR GI frame loop runs 3% faster.
+// spilling out of L1 at 12 warps per SM); here the ReSTIR GI frame loop runs 3% faster.  Five words
+// (kappa computed when a candidate is stored) with four CTAs per SM at 128 registers was slower:
+// 23.7 against 19.9 ms per frame.
 constexpr uint32_t CAND_WORDS = 6;
 constexpr uint32_t CAND_SMEM = CAND_WORDS * NUM_RESAMPLES * WAVE_BLOCK * sizeof(float);
 constexpr uint32_t GUIDE_SHADE_SMEM = CAND_SMEM;  // dynamic shared memory of the guided shade kernel
@@ -481,8 +483,8 @@ LAM_DEV void finalize_records(const Args& A, uint32_t path, v3 scol) {
 template <int Q, bool GUIDE, bool LEARN, bool BATCH>
 // Six CTAs per SM for the unguided forms: the kernel waits on chains of dependent gathers (queue ->
 // hit -> triangle -> material -> texture), so resident warps matter more than the few registers
-// that spill (measured: 79 ms against 87 ms per 16-spp step at 1080p).  The Markov-guided form keeps
-// its registers (156 with its candidate loops rolled; 1 KB of spill at 80).
+// that spill (measured: 79 ms against 87 ms per 16-spp step at 1080p).  The Markov-guided forms keep
+// their registers (160; three CTAs per SM, which their shared-memory candidates also allow).
 __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(const __grid_constant__ Args A) {
     const uint32_t n = *A.count_in;
     const uint32_t lane = threadIdx.x & 31u;
@@ -490,6 +492,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
     G.world = A.world;
     G.old_world = A.old_world;
     G.len = A.world_len;
+    G.mod_m = A.world_mod_m;
     G.camera_loc = A.camera_pos;
     const bool rec = A.ort != nullptr;
     for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;; base += gridDim.x * blockDim.x) {
@@ -764,7 +767,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                             for (int k = 0; k < NUM_RESAMPLES; ++k) {
                                 if (!(cand.weight(k) > 0.0f)) continue;
                                 const MC ck = cand.get(k);
-                                mix_pdf += vmf_pdf(normalize(light_dir(ck, ro)), get_kappa(ck), dir) *
+                                mix_pdf += vmf_pdf_fast(normalize(light_dir(ck, ro)), get_kappa(ck), dir) *
                                            (ck.weight_sum / sum_mc);
                             }
                         }
@@ -791,7 +794,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                                 const float wk = use ? c1 * (ck.weight_sum / sum_mc) : 0.0f;
                                 lobe[k] = make_float4(mean.x, mean.y, mean.z, kappa);
                                 lw[k] = wk;
-                                if (use) pref += wk * vmf_pdf(mean, kappa, dir);
+                                if (use) pref += wk * vmf_pdf_fast(mean, kappa, dir);
                             }
                             A.def_n[path] = make_float4(is.normal.x, is.normal.y, is.normal.z, is.roughness.x);
                             A.def_t[path] = make_float4(is.tangent.x, is.tangent.y, is.tangent.z, __uint_as_float(seed));
@@ -926,7 +929,7 @@ LAM_DEV float markov_mixture_pdf(const Args& A, uint32_t path, float c0, v3 n, v
         const float wk = lw[k];
         if (wk != 0.0f) {
             const float4 l = lobe[k];
-            p += wk * vmf_pdf(mk(l.x, l.y, l.z), l.w, w);
+            p += wk * vmf_pdf_fast(mk(l.x, l.y, l.z), l.w, w);
         }
     }
     return p;
@@ -1845,6 +1848,7 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
     A.world = (uint32_t*)b->world;
     A.old_world = (const uint32_t*)b->old_world;
     A.world_len = b->world_len;
+    A.world_mod_m = ~0ull / std::max<uint64_t>(1, b->world_len) + 1ull;  // grid_index's remainder multiplier
     A.reservoirs = (lam_reservoir*)b->reservoirs;
     if (b->reservoir_len < w->npix) A.reservoirs = nullptr;
     A.info = (lam_info*)b->info;

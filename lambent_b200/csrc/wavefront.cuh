@@ -65,6 +65,7 @@ struct Args {
     uint32_t* world;
     const uint32_t* old_world;
     uint64_t world_len;
+    uint64_t world_mod_m;    // ~0 / world_len + 1: multiplier of the fast remainder that indexes the grid
     lam_reservoir* reservoirs;
     lam_info* info;
     uint32_t* pixel_seed;
