@@ -62,6 +62,9 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--out", default=None, help="also write the JSON line to this file")
+    p.add_argument("--shade-order", default="auto", choices=["auto", "queue", "material"],
+                   help="shade each bounce's hits in traversal order, sorted by shading class, or the "
+                        "library's default (sorted except under Markov guiding)")
     p.add_argument("--no-guided", action="store_true", help="skip the guided-vs-plain equal-time measurement")
     p.add_argument("--guided-only", action="store_true", help="run only the guided-vs-plain measurement")
     p.add_argument("--guided-width", type=int, default=1920)
@@ -95,6 +98,7 @@ def workload_config(a):
         "max_depth": a.depth,
         "textures": f"3 x 16 layers {a.tex}^2 RGBA8 value noise",
         "cache": "inputs larger than L2: path state + textures + triangles exceed 126 MB",
+        "shade_order": a.shade_order,
     }
 
 
@@ -232,6 +236,15 @@ def run_reference(a):
     emit(line, a)
 
 
+def ordered(pipe, a):
+    """Applies --shade-order to a new pipeline."""
+    import lambent_b200 as lb
+    from lambent_b200 import _abi
+    pipe.set_shade_order({"auto": _abi.SHADE_ORDER_AUTO, "queue": _abi.SHADE_ORDER_QUEUE,
+                          "material": _abi.SHADE_ORDER_MATERIAL}[a.shade_order])
+    return pipe
+
+
 def emit(line, a):
     s = json.dumps(line)
     print(s, flush=True)
@@ -262,8 +275,8 @@ def guided_equal_time(a, dev):
     stream = torch.cuda.current_stream()
 
     def pipe(samples, mode=_abi.GUIDE_NONE, guide=None):
-        p = lb.RayTracer(lb.path_tracing.Medium).create_pipeline(*s.layout_counts(), lb.PathTracerOpts(
-            samples=samples, restir_temporal=_abi.RESTIR_DISABLED, max_depth=a.guided_depth, guide_mode=mode))
+        p = ordered(lb.RayTracer(lb.path_tracing.Medium).create_pipeline(*s.layout_counts(), lb.PathTracerOpts(
+            samples=samples, restir_temporal=_abi.RESTIR_DISABLED, max_depth=a.guided_depth, guide_mode=mode)), a)
         if guide is not None:
             p.set_guide(guide)
         return p
@@ -384,8 +397,8 @@ def restir_frames(a, dev):
     gs = lb.GpuScene(s)
     world = 1_500_000
     bufs = lb.DataBuffers(W, H, world, _abi.BUFFER_ALL)
-    pipe = lb.RayTracer(lb.path_tracing.Medium).create_pipeline(*s.layout_counts(), lb.PathTracerOpts(
-        samples=1, restir_temporal=_abi.RESTIR_PER_PIXEL, max_depth=8, guide_mode=_abi.GUIDE_MARKOV))
+    pipe = ordered(lb.RayTracer(lb.path_tracing.Medium).create_pipeline(*s.layout_counts(), lb.PathTracerOpts(
+        samples=1, restir_temporal=_abi.RESTIR_PER_PIXEL, max_depth=8, guide_mode=_abi.GUIDE_MARKOV)), a)
     col = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)
     tg = lb.targets_from(col)
     stream = torch.cuda.current_stream()
@@ -437,7 +450,7 @@ def restir_frames(a, dev):
     equal_time = restir_equal_time(a, dev, s, gs, pipe, col, tg, cams, ms / n)
     return {"config": {"workload": f"Cornell box (36 tris), {W}x{H}, {n}-frame orbit, 1 spp/frame, depth 8, "
                                    "Medium, per-pixel reservoirs, Markov chains (1.5M world cells), temporal + "
-                                   "spatial (5 samples, 61-px window), M cap 20"},
+                                   "spatial (5 samples, 61-px window), M cap 20", "shade_order": a.shade_order},
             "equal_time": equal_time,
             "frames": n, "ms_per_frame": round(ms / n, 3), "frames_per_s": round(n / (ms / 1e3), 2),
             "render_mrays_per_s": round(segs_per_frame / (split[0] / 8 / 1e3) / 1e6, 1),
@@ -473,8 +486,8 @@ def restir_equal_time(a, dev, s, gs, pipe, col, tg, cams, frame_ms):
     plain_bufs = lb.DataBuffers(W, H, 1, 0)
 
     def plain_pipe(spp):
-        return lb.RayTracer(lb.path_tracing.Medium).create_pipeline(*s.layout_counts(), lb.PathTracerOpts(
-            samples=spp, restir_temporal=_abi.RESTIR_DISABLED, max_depth=8, guide_mode=_abi.GUIDE_NONE))
+        return ordered(lb.RayTracer(lb.path_tracing.Medium).create_pipeline(*s.layout_counts(), lb.PathTracerOpts(
+            samples=spp, restir_temporal=_abi.RESTIR_DISABLED, max_depth=8, guide_mode=_abi.GUIDE_NONE)), a)
 
     # plain time per sample at this resolution (after a warm-up call)
     p16 = plain_pipe(16)
@@ -683,7 +696,7 @@ def run_ours(a):
     tracer = lb.RayTracer(lb.path_tracing.Medium)
     opts = lb.PathTracerOpts(samples=a.spp, restir_temporal=lb.RestirTemporalMode.Disabled, max_depth=a.depth,
                              guide_mode=lb.GuideMode.NONE)
-    pipe = tracer.create_pipeline(*scene.layout_counts(), opts)
+    pipe = ordered(tracer.create_pipeline(*scene.layout_counts(), opts), a)
     bufs = lb.DataBuffers(a.width, a.height, 1, 0)
     H, W = a.height, a.width
     color = torch.zeros((H, W, 4), dtype=torch.float32, device=dev)

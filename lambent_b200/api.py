@@ -86,6 +86,7 @@ def lib():
     _sig(L, "lam_render_stats_get", i, vp, P(RenderStats))
     _sig(L, "lam_pipeline_set_profiling", i, vp, i)
     _sig(L, "lam_pipeline_set_wave_paths", i, vp, C.c_uint64)
+    _sig(L, "lam_pipeline_set_shade_order", i, vp, C.c_uint32)
     _sig(L, "lam_render_profile_get", i, vp, P(_abi.StageTimes))
     _sig(L, "lam_render_profile_reset", i, vp)
     _sig(L, "lam_temporal_resampling", i, vp, u32, u32, u32, vp)
@@ -432,6 +433,12 @@ class Pipeline:
     def set_wave_paths(self, max_paths=0):
         """Bounds the paths of one wave (device memory ~220 B per path); 0 restores the default."""
         check(lib().lam_pipeline_set_wave_paths(self._h, int(max_paths)))
+
+    def set_shade_order(self, order=_abi.SHADE_ORDER_AUTO):
+        """SHADE_ORDER_MATERIAL sorts each bounce's hits by class (sky, diffuse, metallic,
+        transparent) before shading; SHADE_ORDER_QUEUE shades them in traversal order;
+        SHADE_ORDER_AUTO (the default) sorts except under Markov guiding."""
+        check(lib().lam_pipeline_set_shade_order(self._h, int(order)))
 
     def profile(self):
         t = _abi.StageTimes()

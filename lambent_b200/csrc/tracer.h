@@ -71,6 +71,7 @@ struct lam_pipeline {
     uint64_t total_segments = 0;
     lam_guide* guide = nullptr;  // learned guide (not owned)
     uint64_t wave_paths = 0;     // bound on the paths of one wave (0: about 32M)
+    uint32_t shade_order = LAM_SHADE_ORDER_AUTO;
     std::vector<char> handler_cubin;   // intersection handler linked with the procedural kernels
     lam::HandlerModule* handler = nullptr;  // loaded on first use
     lam::BatchState* batch = nullptr;  // lam_batch_render state

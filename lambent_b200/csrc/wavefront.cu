@@ -243,10 +243,12 @@ struct WaveBuffers {
     float* def_lw = nullptr;
     uint32_t* def_kind = nullptr;                  // DEF_DIFFUSE / DEF_METAL
     float4 *phit_a = nullptr, *phit_b = nullptr;  // procedural hits (allocated on first use)
+    uint8_t* shade_key = nullptr;                  // material-ordered shading (allocated on first use)
+    uint32_t *shade_order = nullptr, *shade_bc = nullptr;
     uint32_t* ctr = nullptr;  // [0..1] queue counts, [2..3] work counters, [4] error flags,
                               // [8..11] segment counters, [12] diffuse-queue count, [13] records
     std::vector<void*> allocs;
-    int sms = 148, grid_extend = 0, grid_shade = 0, grid_guide = 0;
+    int sms = 148, grid_extend = 0, grid_shade = 0, grid_guide = 0, grid_sort = 0;
 };
 
 static void free_wave(WaveBuffers* w) {
@@ -480,6 +482,125 @@ LAM_DEV void finalize_records(const Args& A, uint32_t path, v3 scol) {
     }
 }
 
+// ---------------------------------------------------------------- material-ordered shading
+// A stable counting sort of the queue by shading class.  A warp that holds sky, diffuse, metallic
+// and transparent lanes runs each class's code in turn with the other lanes idle; in class order
+// the warps are uniform but for the last one of each class.  The three kernels split the queue
+// into one contiguous chunk per block: count the classes of the chunk, scan the counts (class
+// major, then block), and write each position to its slot in the order.  Within a class the queue
+// order is kept, so the shade kernel's reads stay nearly sequential.
+
+LAM_DEV uint32_t shade_class(const DevScene& S, uint2 h) {
+    if (h.x == NO_HIT) return SHADE_SKY;
+    const uint32_t prim = __float_as_uint(ld_keep(S.tris + 3u * h.x).w);
+    const uint32_t ty = load_material(S, h.y, prim).tex_idx_attributes_ty >> 16;
+    return ty == TY_METALLIC ? SHADE_METALLIC : (ty == TY_TRANSPARENT ? SHADE_TRANSPARENT : SHADE_DIFFUSE);
+}
+
+// The chunk of queue positions [*beg, *end) of block b of nb (a multiple of the block size).
+LAM_DEV void sort_chunk(uint32_t n, uint32_t b, uint32_t nb, uint32_t* beg, uint32_t* end) {
+    const uint32_t per = (n + nb - 1u) / nb;
+    const uint32_t c = (per + WAVE_BLOCK - 1u) / WAVE_BLOCK * WAVE_BLOCK;
+    *beg = min(n, b * c);
+    *end = min(n, *beg + c);
+}
+
+__global__ void __launch_bounds__(WAVE_BLOCK) shade_keys_kernel(const __grid_constant__ Args A) {
+    __shared__ uint32_t cnt[SHADE_CLASSES];
+    if (threadIdx.x < SHADE_CLASSES) cnt[threadIdx.x] = 0u;
+    __syncthreads();
+    uint32_t beg, end;
+    sort_chunk(*A.count_in, blockIdx.x, gridDim.x, &beg, &end);
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t t = beg; t < end; t += WAVE_BLOCK) {
+        const uint32_t j = t + threadIdx.x;
+        uint32_t k = SHADE_CLASSES;
+        if (j < end) {
+            k = shade_class(A.S, ld_stream(A.hit + j));
+            A.shade_key[j] = (uint8_t)k;
+        }
+#pragma unroll
+        for (uint32_t c = 0; c < SHADE_CLASSES; ++c) {
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, k == c);
+            if (lane == 0u && m) atomicAdd(&cnt[c], (uint32_t)__popc(m));
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < SHADE_CLASSES) A.shade_bc[blockIdx.x * SHADE_CLASSES + threadIdx.x] = cnt[threadIdx.x];
+}
+
+// One block of SORT_BLOCKS_MAX threads: thread b turns block b's counts into its first slot per
+// class (exclusive, class-major: all of class 0, then class 1, ...).
+__global__ void __launch_bounds__(SORT_BLOCKS_MAX) shade_scan_kernel(const __grid_constant__ Args A, uint32_t nb) {
+    __shared__ uint32_t warp_sum[SORT_BLOCKS_MAX / 32];
+    __shared__ uint32_t class_base;
+    const uint32_t b = threadIdx.x, lane = b & 31u, wid = b >> 5;
+    if (b == 0u) class_base = 0u;
+    for (uint32_t c = 0; c < SHADE_CLASSES; ++c) {
+        const uint32_t v = b < nb ? A.shade_bc[b * SHADE_CLASSES + c] : 0u;
+        uint32_t x = v;  // inclusive scan within the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= (uint32_t)o) x += y;
+        }
+        if (lane == 31u) warp_sum[wid] = x;
+        __syncthreads();
+        if (wid == 0u) {
+            uint32_t s = warp_sum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+                if (lane >= (uint32_t)o) s += y;
+            }
+            warp_sum[lane] = s;  // inclusive over warps
+        }
+        __syncthreads();
+        const uint32_t before = (wid ? warp_sum[wid - 1u] : 0u) + x - v;
+        if (b < nb) A.shade_bc[b * SHADE_CLASSES + c] = class_base + before;
+        __syncthreads();
+        if (b == 0u) class_base += warp_sum[SORT_BLOCKS_MAX / 32 - 1];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(WAVE_BLOCK) shade_scatter_kernel(const __grid_constant__ Args A) {
+    constexpr uint32_t NW = WAVE_BLOCK / 32;
+    __shared__ uint32_t wcnt[NW][SHADE_CLASSES];
+    __shared__ uint32_t next[SHADE_CLASSES];
+    if (threadIdx.x < SHADE_CLASSES) next[threadIdx.x] = A.shade_bc[blockIdx.x * SHADE_CLASSES + threadIdx.x];
+    __syncthreads();
+    uint32_t beg, end;
+    sort_chunk(*A.count_in, blockIdx.x, gridDim.x, &beg, &end);
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    const uint32_t below = (1u << lane) - 1u;
+    for (uint32_t t = beg; t < end; t += WAVE_BLOCK) {
+        const uint32_t j = t + threadIdx.x;
+        const uint32_t k = j < end ? (uint32_t)A.shade_key[j] : SHADE_CLASSES;
+        uint32_t rank = 0u;
+#pragma unroll
+        for (uint32_t c = 0; c < SHADE_CLASSES; ++c) {
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, k == c);
+            if (k == c) rank = (uint32_t)__popc(m & below);
+            if (lane == 0u) wcnt[wid][c] = (uint32_t)__popc(m);
+        }
+        __syncthreads();
+        if (k < SHADE_CLASSES) {
+            uint32_t slot = next[k] + rank;
+            for (uint32_t w = 0; w < wid; ++w) slot += wcnt[w][k];
+            A.shade_order[slot] = j;
+        }
+        __syncthreads();
+        if (threadIdx.x < SHADE_CLASSES) {
+            uint32_t add = 0u;
+#pragma unroll
+            for (uint32_t w = 0; w < NW; ++w) add += wcnt[w][threadIdx.x];
+            next[threadIdx.x] += add;
+        }
+        __syncthreads();
+    }
+}
+
 template <int Q, bool GUIDE, bool LEARN, bool BATCH>
 // Six CTAs per SM for the unguided forms: the kernel waits on chains of dependent gathers (queue ->
 // hit -> triangle -> material -> texture), so resident warps matter more than the few registers
@@ -497,15 +618,20 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
     const bool rec = A.ort != nullptr;
     for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;; base += gridDim.x * blockDim.x) {
         if (base >= n) break;
-        const uint32_t i = base + lane;
+        const uint32_t j = base + lane;  // work item; i: the queue position it shades
+        const uint32_t i = (A.shade_order && j < n) ? A.shade_order[j] : j;
         {
             // the next iteration's queue-ordered inputs have known addresses: start them towards L2
-            const uint32_t inext = i + gridDim.x * blockDim.x;
-            if (inext < n) {
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.q_in + inext));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.hit + inext));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.ray_o + inext));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.ray_d + inext));
+            const uint32_t jnext = j + gridDim.x * blockDim.x;
+            if (jnext < n) {
+                if (A.shade_order) {
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(A.shade_order + jnext));
+                } else {
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(A.q_in + jnext));
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(A.hit + jnext));
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(A.ray_o + jnext));
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(A.ray_d + jnext));
+                }
             }
         }
         bool cont = false, deferred = false;
@@ -1445,6 +1571,7 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
     occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_kernel<LAM_QUALITY_MEDIUM, false, false, false>, WAVE_BLOCK, 0);
     w->grid_shade = w->sms * std::max(1, occ);
+    w->grid_sort = std::min(SORT_BLOCKS_MAX, w->sms * 4);
     if (guide) {
         const void* ks[] = {(const void*)shade_kernel<LAM_QUALITY_LOW, true, false, false>,
                             (const void*)shade_kernel<LAM_QUALITY_MEDIUM, true, false, false>,
@@ -1706,6 +1833,14 @@ extern "C" int lam_pipeline_set_wave_paths(lam_pipeline* p, uint64_t max_paths) 
     return LAM_OK;
 }
 
+extern "C" int lam_pipeline_set_shade_order(lam_pipeline* p, uint32_t order) {
+    if (!p) return set_error(LAM_ERR_INVALID_ARGUMENT, "null pipeline");
+    if (order != LAM_SHADE_ORDER_AUTO && order != LAM_SHADE_ORDER_QUEUE && order != LAM_SHADE_ORDER_MATERIAL)
+        return set_error(LAM_ERR_INVALID_ARGUMENT, "unknown shade order");
+    p->shade_order = order;
+    return LAM_OK;
+}
+
 extern "C" int lam_pipeline_set_guide(lam_pipeline* p, lam_guide* g) {
     if (!p) return set_error(LAM_ERR_INVALID_ARGUMENT, "null pipeline");
     p->guide = g;
@@ -1886,6 +2021,15 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         std::memcpy(A.box, s->bounds, sizeof(A.box));
     }
     if (guide && !world) return set_error(LAM_ERR_INVALID_ARGUMENT, "Markov guiding needs MARKOV_CHAIN_WORLD_SPACE buffers");
+    const bool sorted = pl->shade_order == LAM_SHADE_ORDER_MATERIAL || (pl->shade_order == LAM_SHADE_ORDER_AUTO && !guide);
+    if (sorted) {
+        if (!w->shade_order && (walloc(w, &w->shade_key, w->paths) || walloc(w, &w->shade_order, w->paths) ||
+                                walloc(w, &w->shade_bc, (size_t)SORT_BLOCKS_MAX * SHADE_CLASSES)))
+            return LAM_ERR_CUDA;
+        A.shade_key = w->shade_key;
+        A.shade_order = w->shade_order;
+        A.shade_bc = w->shade_bc;
+    }
     const bool alpha = !s->dev.all_opaque;
     const dim3 blk(WAVE_BLOCK);
     const dim3 gpix((w->npix + WAVE_BLOCK - 1) / WAVE_BLOCK);
@@ -1980,6 +2124,12 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
             end(h);
             h = begin(2);
             if (gd) cudaMemsetAsync(w->ctr + 12, 0, sizeof(uint32_t), st);
+            if (sorted) {
+                shade_keys_kernel<<<w->grid_sort, blk, 0, st>>>(A);
+                shade_scan_kernel<<<1, SORT_BLOCKS_MAX, 0, st>>>(A, (uint32_t)w->grid_sort);
+                shade_scatter_kernel<<<w->grid_sort, blk, 0, st>>>(A);
+                launches += 3;
+            }
             switch (pl->quality) {
                 case LAM_QUALITY_LOW: launch_shade<LAM_QUALITY_LOW>(guide, learned, w->grid_shade, blk, st, A); break;
                 case LAM_QUALITY_HIGH: launch_shade<LAM_QUALITY_HIGH>(guide, learned, w->grid_shade, blk, st, A); break;

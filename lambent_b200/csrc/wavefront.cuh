@@ -10,6 +10,10 @@ namespace lam {
 constexpr int WAVE_BLOCK = 128;
 enum : uint32_t { DEF_DIFFUSE = 0u, DEF_METAL = 1u };  // kinds of vertices deferred to the learned guide
 constexpr uint32_t NO_REC = 0xFFFFFFFFu;
+// classes of material-ordered shading: what a bounce runs differs between sky lanes, diffuse,
+// metallic and transparent vertices
+enum : uint32_t { SHADE_SKY = 0u, SHADE_DIFFUSE = 1u, SHADE_METALLIC = 2u, SHADE_TRANSPARENT = 3u, SHADE_CLASSES = 4u };
+constexpr int SORT_BLOCKS_MAX = 1024;  // blocks of the class-count and scatter kernels (one scan block)
 
 // ---------------------------------------------------------------- batched renders
 // A request of lam_batch_render: its scene, camera, image and samples.
@@ -48,6 +52,11 @@ struct Args {
     float4 *qthr_out, *qacc_out;
     uint4* qmisc_out;
     uint2* hit;  // (triangle slot, instance) of the closest hit, by position in the current queue
+    // material-ordered shading (lam_pipeline_set_shade_order): the class of each queued hit, the queue
+    // positions in class order (null: the shade kernel takes them in queue order), and per-block class
+    // counts, which the scan turns into the blocks' first output slots
+    uint8_t* shade_key;
+    uint32_t *shade_order, *shade_bc;
     uint32_t *q_in, *q_out;
     uint32_t *count_in, *count_out, *work;
     uint32_t* err;

@@ -51,6 +51,9 @@ pub const LAM_HIT_FRONT: c_int = 1;
 pub const LAM_HIT_BACK: c_int = 2;
 pub const LAM_TRACE_MAX_RAYS: u32 = 0x7FFFFFFF;
 pub const LAM_TRACE_STATIC_MAX_RAYS: u32 = 0x7FFFFFFF;
+pub const LAM_SHADE_ORDER_AUTO: u32 = 0;
+pub const LAM_SHADE_ORDER_QUEUE: u32 = 1;
+pub const LAM_SHADE_ORDER_MATERIAL: u32 = 2;
 pub const LAM_GUIDE_PARAMS: u32 = 16384;
 pub const LAM_GUIDE_OUTPUTS: u32 = 40;
 
@@ -395,6 +398,7 @@ extern "C" {
     pub fn lam_pipeline_set_profiling(pipeline: *mut lam_pipeline, enabled: c_int) -> c_int;
     pub fn lam_render_profile_get(pipeline: *mut lam_pipeline, out: *mut lam_stage_times) -> c_int;
     pub fn lam_pipeline_set_wave_paths(pipeline: *mut lam_pipeline, max_paths: u64) -> c_int;
+    pub fn lam_pipeline_set_shade_order(pipeline: *mut lam_pipeline, order: u32) -> c_int;
     pub fn lam_render_profile_reset(pipeline: *mut lam_pipeline) -> c_int;
     pub fn lam_temporal_resampling(buffers: *mut lam_data_buffers, width: u32, height: u32, seed_offset: u32, stream: *mut c_void) -> c_int;
     pub fn lam_spatial_resampling(buffers: *mut lam_data_buffers, targets: *const lam_frame_targets, is_samples: u32, is_space: u32, seed_offset: u32, stream: *mut c_void) -> c_int;

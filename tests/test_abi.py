@@ -214,3 +214,4 @@ def test_pipeline_tuning_entry_points_reject_null_pipelines():
     assert L.lam_pipeline_set_wave_paths(None, C.c_uint64(1 << 20)) == _abi.ERR_INVALID_ARGUMENT
     assert L.lam_pipeline_set_profiling(None, 1) == _abi.ERR_INVALID_ARGUMENT
     assert L.lam_pipeline_set_guide(None, None) == _abi.ERR_INVALID_ARGUMENT
+    assert L.lam_pipeline_set_shade_order(None, _abi.SHADE_ORDER_MATERIAL) == _abi.ERR_INVALID_ARGUMENT
