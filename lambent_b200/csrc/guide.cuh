@@ -166,6 +166,47 @@ LAM_DEV MC grid_load(const Grid& g, v3 pos, v3 normal, v3 incoming, bool force_o
     return s;
 }
 
+// grid_load of N cells (the world-space candidates of one bounce, general.wesl:389-398): every
+// cell's words are read before any of them is examined, so the N reads are in flight together
+// instead of one after another.  A cell's own words are read in grid_load's order.  When two
+// candidates hash to one cell, the second read no longer sees the first one's timeout refresh;
+// that refresh writes the value the word then holds, and the chain fields it returns are the same.
+// Measured on the ReSTIR GI frame loop at 1080p: 19.45 / 19.86 against 20.03 / 20.22 ms per frame.
+template <int N>
+LAM_DEV void grid_load_n(const Grid& g, const v3* pos, v3 normal, v3 incoming, const bool* force_old, MC* out) {
+    uint32_t* e[N];
+    uint64_t idx[N];
+    uint32_t sec[N], tmo[N], tag[N];
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+        IVec l = grid_loc(g, pos[q]);
+        idx[q] = grid_index(g, primary_hash(l, normal, incoming));
+        e[q] = g.world + idx[q] * W_STRIDE;
+        sec[q] = secondary_hash(l, normal);
+    }
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+        out[q] = read_chain_timeout(e[q], &tmo[q]);
+        tag[q] = vload(e[q] + W_SEC);
+    }
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+        MC s = out[q];
+        if (tag[q] != sec[q] || force_old[q]) {
+            const uint32_t* o = g.old_world ? g.old_world + idx[q] * W_STRIDE : nullptr;
+            if (o && vload(o + W_SEC) == sec[q]) s = read_chain(o);
+            else s = mc_zero();
+        } else if (tmo[q] != CACHE_TIMEOUT) {
+            vstore(e[q] + W_TIMEOUT, CACHE_TIMEOUT);
+        }
+        s.light = strip_nan3(s.light);
+        s.mean_cosine = strip_nan(s.mean_cosine);
+        s.weight_sum = strip_nan(s.weight_sum);
+        s.score = strip_nan(s.score);
+        out[q] = s;
+    }
+}
+
 LAM_DEV void grid_store(const Grid& g, v3 pos, v3 normal, v3 incoming, const MC& st) {
     IVec l = grid_loc(g, pos);
     uint64_t idx = grid_index(g, primary_hash(l, normal, incoming));

@@ -810,21 +810,32 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 MC s = mc_zero();
                 if (GUIDE) {
                     screen_candidates(A, pixel, __float_as_uint(pn.w), cand);
-                    // the candidate loops stay rolled: the guided kernel is large, and unrolled it
-                    // needs 222 registers (2 CTAs per SM) and stalls on instruction fetch
-#pragma unroll 1
-                    for (int k = 16; k < 20; ++k) {
-                        bool rc = rand_f32(seed) < 0.7f;
-                        float jm = rc ? 0.75f : 1.0f;
-                        float j0 = rand_f32_ptr(&seed);
-                        float j1 = rand_f32_ptr(&seed);
-                        v3 jit = (mk(j0, 0.0f, j1) * 0.15000000596046448f) * jm;
-                        cand.put(k, grid_load(G, ro + from_onb_no_tangent(jit, is.normal), is.normal, rd, rc));
-                        seed += 1u;
+                    // the four world-space candidates: their jittered positions first (the seed
+                    // advances as in general.wesl:390-398), then their cells' reads together
+                    {
+                        v3 wpos[4];
+                        bool wold[4];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            bool rc = rand_f32(seed) < 0.7f;
+                            float jm = rc ? 0.75f : 1.0f;
+                            float j0 = rand_f32_ptr(&seed);
+                            float j1 = rand_f32_ptr(&seed);
+                            v3 jit = (mk(j0, 0.0f, j1) * 0.15000000596046448f) * jm;
+                            wpos[q] = ro + from_onb_no_tangent(jit, is.normal);
+                            wold[q] = rc;
+                            seed += 1u;
+                        }
+                        MC wc[4];
+                        grid_load_n<4>(G, wpos, is.normal, rd, wold, wc);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) cand.put(16 + q, wc[q]);
                     }
                     cand.put(20, tentative);
                     sum_mc = 0.0f;
                     int sel = -1;
+                    // the resampling loop stays rolled: the guided kernel is large, and unrolled its
+                    // candidate loops needed 222 registers (2 CTAs per SM) and stalled on instruction fetch
 #pragma unroll 1
                     for (int k = 0; k < NUM_RESAMPLES; ++k) {
                         seed = rand_u32(seed);
