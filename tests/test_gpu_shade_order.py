@@ -56,6 +56,30 @@ def test_material_order_across_waves_on_the_instanced_field(cuda):
     assert a["stats"].ray_segments == b["stats"].ray_segments
 
 
+def test_material_order_with_an_intersection_handler(cuda):
+    """Procedural spheres through the run-time-linked extend kernel and the handler's normals: the
+    sort classes procedural hits by their instance's material like triangle hits, and the image is
+    the same either way."""
+    import os
+    import torch
+    src = open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "sphere_handler.cu")).read()
+    s = scenes.with_spheres(scenes.cornell_box(64, 64), n=48, seed=3)
+    g = lb.GpuScene(s)
+    out = []
+    for order in (QUEUE, MATERIAL):
+        t = lb.RayTracer(lb.path_tracing.Medium)
+        t.set_intersection_handler(src)
+        pipe = t.create_pipeline(*s.layout_counts(), lb.PathTracerOpts(
+            samples=8, restir_temporal=_abi.RESTIR_DISABLED, max_depth=5))
+        pipe.set_shade_order(order)
+        col = torch.zeros((s.height, s.width, 4), dtype=torch.float32, device="cuda")
+        pipe.render(g, lb.DataBuffers(s.width, s.height, 1, 0), s.camera, lb.targets_from(col), 7)
+        torch.cuda.synchronize()
+        assert pipe.stats().error_flags == 0
+        out.append(col.cpu().numpy())
+    np.testing.assert_array_equal(out[0], out[1])
+
+
 def test_material_order_matches_oracle(cuda):
     """The sorted render against the oracle, with the same-seed bound of the queue-ordered test."""
     s = scenes.cornell_box(64, 64)
