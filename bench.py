@@ -523,17 +523,20 @@ def restir_equal_time(a, dev, s, gs, pipe, col, tg, cams, frame_ms):
         # relMSE is a mean of squares: a few firefly pixels can dominate it, so the share of pixels whose
         # squared relative error exceeds 100 (error > 10x the reference) is reported beside it
         # (and the part of the relMSE sum that those pixels carry)
+        # and the median pixel's squared relative error, which the few fireflies do not move
         def fireflies(img):
             sq = ((img - ref) ** 2) / den
             hot = sq.max(-1)[0] > 100.0
-            return float(hot.double().mean()), float(sq[hot].sum() / sq.sum().clamp_min(1e-30))
-        fire_r, carried_r = fireflies(kept[f])
-        fire_p, carried_p = fireflies(plain)
+            return (float(hot.double().mean()), float(sq[hot].sum() / sq.sum().clamp_min(1e-30)),
+                    float(sq.mean(-1).median()))
+        fire_r, carried_r, med_r = fireflies(kept[f])
+        fire_p, carried_p, med_p = fireflies(plain)
         rows.append({"frame": f, "restir_relmse": round(e_restir, 6), "plain_relmse": round(e_plain, 6),
                      "ratio": round(e_restir / e_plain, 4) if e_plain > 0 else None,
                      "ref_noise_relmse": round(noise, 7),
                      "firefly_pixel_share": {"restir": round(fire_r, 7), "plain": round(fire_p, 7)},
-                     "firefly_relmse_share": {"restir": round(carried_r, 4), "plain": round(carried_p, 4)}})
+                     "firefly_relmse_share": {"restir": round(carried_r, 4), "plain": round(carried_p, 4)},
+                     "median_pixel_relse": {"restir": round(med_r, 6), "plain": round(med_p, 6)}})
     torch.cuda.synchronize()
     ratios = sorted(r["ratio"] for r in rows if r["ratio"] is not None)
     return {"plain_spp_at_equal_time": spp_eq, "plain_ms_per_spp": round(ms_per_spp, 4),

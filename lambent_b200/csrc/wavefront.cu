@@ -505,6 +505,8 @@ LAM_DEV void sort_chunk(uint32_t n, uint32_t b, uint32_t nb, uint32_t* beg, uint
     *end = min(n, *beg + c);
 }
 
+// BATCH: each path's scene is its request's (lam_batch_render).
+template <bool BATCH>
 __global__ void __launch_bounds__(WAVE_BLOCK) shade_keys_kernel(const __grid_constant__ Args A) {
     __shared__ uint32_t cnt[SHADE_CLASSES];
     if (threadIdx.x < SHADE_CLASSES) cnt[threadIdx.x] = 0u;
@@ -516,7 +518,10 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_keys_kernel(const __grid_con
         const uint32_t j = t + threadIdx.x;
         uint32_t k = SHADE_CLASSES;
         if (j < end) {
-            k = shade_class(A.S, ld_stream(A.hit + j));
+            // plain loads: the shade kernel reads the hit (and a batched path's flags) again next
+            const DevScene* S = &A.S;
+            if (BATCH) S = &A.reqs[A.segs[A.qmisc[j].z >> 16].req].S;
+            k = shade_class(*S, A.hit[j]);
             A.shade_key[j] = (uint8_t)k;
         }
 #pragma unroll
@@ -1582,7 +1587,7 @@ static int ensure_wave(lam_pipeline* pl, uint32_t width, uint32_t height, bool f
     occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, shade_kernel<LAM_QUALITY_MEDIUM, false, false, false>, WAVE_BLOCK, 0);
     w->grid_shade = w->sms * std::max(1, occ);
-    w->grid_sort = std::min(SORT_BLOCKS_MAX, w->sms * 4);
+    w->grid_sort = std::min(SORT_BLOCKS_MAX, w->sms * 6);
     if (guide) {
         const void* ks[] = {(const void*)shade_kernel<LAM_QUALITY_LOW, true, false, false>,
                             (const void*)shade_kernel<LAM_QUALITY_MEDIUM, true, false, false>,
@@ -2136,7 +2141,7 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
             h = begin(2);
             if (gd) cudaMemsetAsync(w->ctr + 12, 0, sizeof(uint32_t), st);
             if (sorted) {
-                shade_keys_kernel<<<w->grid_sort, blk, 0, st>>>(A);
+                shade_keys_kernel<false><<<w->grid_sort, blk, 0, st>>>(A);
                 shade_scan_kernel<<<1, SORT_BLOCKS_MAX, 0, st>>>(A, (uint32_t)w->grid_sort);
                 shade_scatter_kernel<<<w->grid_sort, blk, 0, st>>>(A);
                 launches += 3;
@@ -2343,13 +2348,15 @@ static int batch_wave_buffers(BatchState* b, uint32_t capacity) {
 }
 
 static void batch_key(const lam_batch_request* r, uint32_t n, const lam_batch_tuning& t, uint64_t generation,
-                      std::vector<char>& key) {
-    key.resize(sizeof(uint32_t) + n * sizeof(lam_batch_request) + sizeof(t) + sizeof(generation));
+                      bool sorted, std::vector<char>& key) {
+    const size_t base = sizeof(uint32_t) + n * sizeof(lam_batch_request) + sizeof(t) + sizeof(generation);
+    key.resize(base + 1);
     char* k = key.data();
     std::memcpy(k, &n, sizeof(n));
     std::memcpy(k + sizeof(n), r, n * sizeof(lam_batch_request));
     std::memcpy(k + sizeof(n) + n * sizeof(lam_batch_request), &t, sizeof(t));
     std::memcpy(k + sizeof(n) + n * sizeof(lam_batch_request) + sizeof(t), &generation, sizeof(generation));
+    k[base] = sorted ? 1 : 0;
 }
 
 }  // namespace lam
@@ -2399,6 +2406,15 @@ extern "C" int lam_batch_render(lam_pipeline* pl, const lam_batch_request* reqs,
                                                           : (uint32_t)std::max(1, occ_e));
     const int grid_s = sms * (int)(t.shade_blocks_per_sm ? t.shade_blocks_per_sm : (uint32_t)std::max(1, occ_s));
     const BatchPlan P = plan_batch(reqs, n, t.wave_paths);
+    // material-ordered shading (no Markov guiding here, so the automatic order sorts)
+    const bool sorted = pl->shade_order != LAM_SHADE_ORDER_QUEUE;
+    const int grid_sort = std::min(SORT_BLOCKS_MAX, sms * 6);
+    if (sorted && !w->shade_order) {
+        b->generation++;  // a captured graph does not know the new buffers
+        if (walloc(w, &w->shade_key, b->capacity) || walloc(w, &w->shade_order, b->capacity) ||
+            walloc(w, &w->shade_bc, (size_t)SORT_BLOCKS_MAX * SHADE_CLASSES))
+            return LAM_ERR_CUDA;
+    }
     // device tables (uploaded before any capture)
     if (dgrow(b, &b->reqs, &b->reqs_cap, n) || dgrow(b, &b->segs, &b->segs_cap, P.segs.size()) ||
         dgrow(b, &b->done, &b->done_cap, n) || dgrow(b, &b->times, &b->times_cap, n + 1) ||
@@ -2457,6 +2473,11 @@ extern "C" int lam_batch_render(lam_pipeline* pl, const lam_batch_request* reqs,
     A.reqs = b->reqs;
     A.req_done = b->done;
     A.req_time = b->times;
+    if (sorted) {
+        A.shade_key = w->shade_key;
+        A.shade_order = w->shade_order;
+        A.shade_bc = w->shade_bc;
+    }
     const dim3 blk(WAVE_BLOCK);
     uint32_t launches = 0;
     auto record = [&]() {
@@ -2503,6 +2524,12 @@ extern "C" int lam_batch_render(lam_pipeline* pl, const lam_batch_request* reqs,
                 cudaMemsetAsync(cb, 0, sizeof(uint32_t), st);
                 if (all_opaque) extend_batch_kernel<false><<<grid_e, blk, 0, st>>>(A);
                 else extend_batch_kernel<true><<<grid_e, blk, 0, st>>>(A);
+                if (sorted) {
+                    shade_keys_kernel<true><<<grid_sort, blk, 0, st>>>(A);
+                    shade_scan_kernel<<<1, SORT_BLOCKS_MAX, 0, st>>>(A, (uint32_t)grid_sort);
+                    shade_scatter_kernel<<<grid_sort, blk, 0, st>>>(A);
+                    launches += 3;
+                }
                 switch (pl->quality) {
                     case LAM_QUALITY_LOW: shade_kernel<LAM_QUALITY_LOW, false, false, true><<<grid_s, blk, 0, st>>>(A); break;
                     case LAM_QUALITY_HIGH: shade_kernel<LAM_QUALITY_HIGH, false, false, true><<<grid_s, blk, 0, st>>>(A); break;
@@ -2523,7 +2550,7 @@ extern "C" int lam_batch_render(lam_pipeline* pl, const lam_batch_request* reqs,
     };
     if (t.use_graph) {
         std::vector<char> key;
-        batch_key(reqs, n, t, b->generation, key);
+        batch_key(reqs, n, t, b->generation, sorted, key);
         if (!b->graph || key != b->graph_key) {
             if (b->graph) cudaGraphExecDestroy(b->graph);
             b->graph = nullptr;

@@ -38,6 +38,9 @@ def _single(req, torch):
 
 @pytest.mark.parametrize("graph", [0, 1])
 def test_batch_matches_single_renders(cuda, graph):
+    """Two calls on one pipeline, the first in material order (the default) and the second in
+    queue order: a captured graph is rebuilt when the order changes, and either order renders
+    each request exactly as lam_render does."""
     import torch
     reqs = _requests(torch)
     pipe = _pipe(reqs[0]["scene"])
@@ -45,7 +48,8 @@ def test_batch_matches_single_renders(cuda, graph):
     # a small queue forces several waves and splits the largest request's samples across them
     tuning = _abi.BatchTuning(wave_paths=64 * 1024, use_graph=graph)
     refs = [_single(r, torch) for r in reqs]
-    for call in range(2):
+    for call, order in enumerate((_abi.SHADE_ORDER_AUTO, _abi.SHADE_ORDER_QUEUE)):
+        pipe.set_shade_order(order)
         for r in reqs:
             r["col"].zero_()
         pipe.batch_render(batch, tuning)
