@@ -237,7 +237,7 @@ struct WaveBuffers {
     // learned guiding: deferred diffuse vertices and the per-path training-record lists
     bool learned = false;
     uint32_t* dq = nullptr;
-    float4 *def_n = nullptr, *def_t = nullptr, *def_c = nullptr, *def_o = nullptr, *def_d = nullptr;
+    float4 *def_n = nullptr, *def_t = nullptr, *def_c = nullptr, *def_o = nullptr, *def_d = nullptr, *def_a = nullptr;
     uint32_t* rec_head = nullptr;
     float4 *def_r = nullptr, *def_lobe = nullptr;  // the Markov sampler's or the metal's draw; Markov lobes
     float* def_lw = nullptr;
@@ -1002,16 +1002,9 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
             o_acc = make_float4(scol.x, scol.y, scol.z, cached_pdf);
             o_misc = make_uint4(__float_as_uint(cached_brdf), seed, nfl, 0u);
             // a finished path leaves its radiance by path for the accumulate kernel; a deferred one its
-            // whole state for the guide kernel; a continuing one goes with its queue slot (below)
-            if (!cont || deferred) A.acc[path] = o_acc;
-            if (deferred) {
-                A.thr[path] = o_thr;
-                A.brdf[path] = cached_brdf;
-                A.seed[path] = seed;
-                A.flags[path] = nfl;
-                A.def_o[path] = make_float4(ro.x, ro.y, ro.z, 0.0f);
-                A.def_d[path] = make_float4(rd.x, rd.y, rd.z, 0.0f);
-            }
+            // live state at its slot in the guide kernel's queue, and a continuing one its state at its
+            // slot in the next queue (both below)
+            if (!cont) A.acc[path] = o_acc;
             if (rec) {
                 A.ort[path] = make_float4(orc.x, orc.y, orc.z, sum_mc);
                 A.orad[path] = make_float4(orad.x, orad.y, orad.z, 0.0f);
@@ -1024,7 +1017,28 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 mc_store(A.tent_live + pixel, tentative);
             }
         }
-        // warp-aggregated append of the surviving paths (deferred ones go to the guide kernel's queue)
+        // warp-aggregated appends of the surviving paths: deferred ones to the guide kernel's queue, with
+        // their live state at their slot there (the guide kernel reads it in queue order), the others
+        // to the next queue
+        if (LEARN) {
+            const uint32_t dmask = __ballot_sync(0xFFFFFFFFu, deferred);
+            if (dmask) {
+                uint32_t slot = 0;
+                if (lane == 0) slot = atomicAdd(A.dq_count, __popc(dmask));
+                slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
+                if (deferred) {
+                    const uint32_t q = slot + __popc(dmask & ((1u << lane) - 1u));
+                    A.dq[q] = path;
+                    A.def_o[q] = make_float4(ro.x, ro.y, ro.z, 0.0f);
+                    A.def_d[q] = make_float4(rd.x, rd.y, rd.z, 0.0f);
+                    A.thr[q] = o_thr;
+                    A.def_a[q] = o_acc;
+                    A.brdf[q] = __uint_as_float(o_misc.x);
+                    A.seed[q] = o_misc.y;
+                    A.flags[q] = o_misc.z;
+                }
+            }
+        }
         const bool next = cont && !deferred;
         const uint32_t mask = __ballot_sync(0xFFFFFFFFu, next);
         if (mask) {
@@ -1039,15 +1053,6 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                 A.qthr_out[s] = o_thr;
                 A.qacc_out[s] = o_acc;
                 A.qmisc_out[s] = o_misc;
-            }
-        }
-        if (LEARN) {
-            const uint32_t dmask = __ballot_sync(0xFFFFFFFFu, deferred);
-            if (dmask) {
-                uint32_t slot = 0;
-                if (lane == 0) slot = atomicAdd(A.dq_count, __popc(dmask));
-                slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
-                if (deferred) A.dq[slot + __popc(dmask & ((1u << lane) - 1u))] = path;
             }
         }
     }
@@ -1107,11 +1112,11 @@ LAM_DEV void record_vertex(const Args& A, uint32_t path, uint32_t seed0, v3 ro, 
 // times the cosine equals the albedo times p_metal).  Untrained (NET false) it is the reference's
 // bounce, unchanged.
 template <bool NET, bool MARKOV>
-LAM_DEV void guide_finish_metal(const Args& A, uint32_t path, const net::Lobes* L) {
-    const float4 d4 = A.def_d[path], dn = A.def_n[path], dt = A.def_t[path], dr = A.def_r[path];
+LAM_DEV void guide_finish_metal(const Args& A, uint32_t q, uint32_t path, const net::Lobes* L) {
+    const float4 d4 = A.def_d[q], dn = A.def_n[path], dt = A.def_t[path], dr = A.def_r[path];
     v3 dir = mk(dr.x, dr.y, dr.z);
     if (NET) {
-        const float4 th = A.thr[path];
+        const float4 th = A.thr[q];
         const v3 rd = mk(d4.x, d4.y, d4.z), n = mk(dn.x, dn.y, dn.z), t = mk(dt.x, dt.y, dt.z);
         const uint32_t seed0 = __float_as_uint(dt.w);
         const float f = A.guide_frac;
@@ -1128,24 +1133,27 @@ LAM_DEV void guide_finish_metal(const Args& A, uint32_t path, const net::Lobes* 
         const float pm = metal_pdf(rd, n, t, dn.w, dr.w, dir);
         const float mix = (1.0f - f) * pm + f * net::mixture_pdf(*L, dir);
         const float wgt = mix > 0.0f ? pm / mix : 0.0f;
-        A.thr[path] = make_float4(th.x * wgt, th.y * wgt, th.z * wgt, th.w);
+        A.thr[q] = make_float4(th.x * wgt, th.y * wgt, th.z * wgt, th.w);
         if (MARKOV) {
             const float4 oc = A.ort[path];
             A.ort[path] = make_float4(oc.x * wgt, oc.y * wgt, oc.z * wgt, oc.w);
         }
     }
-    A.def_d[path] = make_float4(dir.x, dir.y, dir.z, 0.0f);
+    A.def_d[q] = make_float4(dir.x, dir.y, dir.z, 0.0f);
 }
 
+// The vertex at guide queue slot q of path `path`: its live state (origin, direction, throughput,
+// sample colour, brdf, seed, flags) is stored by slot, what the shade kernel decided at the vertex
+// (kind, frame, albedo, the Markov draw and lobes) by path, as are its training records.
 template <int Q, bool NET, bool MARKOV>
-LAM_DEV void guide_finish(const Args& A, uint32_t path, const net::Lobes* L, bool& out) {
+LAM_DEV void guide_finish(const Args& A, uint32_t q, uint32_t path, const net::Lobes* L, bool& out) {
     if (A.def_kind[path] == DEF_METAL) {
-        guide_finish_metal<NET, MARKOV>(A, path, L);
+        guide_finish_metal<NET, MARKOV>(A, q, path, L);
         out = true;
         return;
     }
-    const float4 o4 = A.def_o[path], d4 = A.def_d[path], dn = A.def_n[path], dt = A.def_t[path], dc = A.def_c[path];
-    const float4 th = A.thr[path], ac = A.acc[path];
+    const float4 o4 = A.def_o[q], d4 = A.def_d[q], dn = A.def_n[path], dt = A.def_t[path], dc = A.def_c[path];
+    const float4 th = A.thr[q], ac = A.def_a[q];
     const v3 ro = mk(o4.x, o4.y, o4.z), rd = mk(d4.x, d4.y, d4.z), n = mk(dn.x, dn.y, dn.z), t = mk(dt.x, dt.y, dt.z);
     const uint32_t seed0 = __float_as_uint(dt.w);
     v3 color = mk(th.x, th.y, th.z);
@@ -1168,7 +1176,7 @@ LAM_DEV void guide_finish(const Args& A, uint32_t path, const net::Lobes* L, boo
                 const float u2 = rand_f32(h);
                 dir = net::mixture_sample(*L, u0, u1, u2);
                 pdf = markov_mixture_pdf(A, path, dc.w, n, dir);
-                A.flags[path] |= 0x100u;  // not drawn from a chain's vMF lobe (general.wesl:469-472)
+                A.flags[q] |= 0x100u;  // not drawn from a chain's vMF lobe (general.wesl:469-472)
             }
             pdf = (1.0f - f) * pdf + f * net::mixture_pdf(*L, dir);
         }
@@ -1203,10 +1211,10 @@ LAM_DEV void guide_finish(const Args& A, uint32_t path, const net::Lobes* L, boo
         const v3 orc = (mk(oc.x, oc.y, oc.z) * nf) * diffuse;
         A.ort[path] = make_float4(orc.x, orc.y, orc.z, oc.w);
     }
-    A.thr[path] = make_float4(color.x, color.y, color.z, th.w);
-    A.brdf[path] = cached_brdf;
-    A.acc[path] = make_float4(ac.x, ac.y, ac.z, pdf);
-    A.def_d[path] = make_float4(dir.x, dir.y, dir.z, 0.0f);
+    A.thr[q] = make_float4(color.x, color.y, color.z, th.w);
+    A.brdf[q] = cached_brdf;
+    A.def_a[q] = make_float4(ac.x, ac.y, ac.z, pdf);
+    A.def_d[q] = make_float4(dir.x, dir.y, dir.z, 0.0f);
     record_vertex(A, path, seed0, ro, n, rd, dir, color_pre, ac);
     out = true;
 }
@@ -1222,7 +1230,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
             uint32_t path = 0;
             if (i < n) {
                 path = A.dq[i];
-                guide_finish<Q, false, MARKOV>(A, path, nullptr, go);
+                guide_finish<Q, false, MARKOV>(A, i, path, nullptr, go);
             }
             const uint32_t mask = __ballot_sync(0xFFFFFFFFu, go);
             uint32_t slot = 0;
@@ -1231,11 +1239,11 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
             if (go) {
                 const uint32_t s = slot + __popc(mask & ((1u << lane) - 1u));
                 A.q_out[s] = path;
-                A.ray_o_out[s] = A.def_o[path];
-                A.ray_d_out[s] = A.def_d[path];
-                A.qthr_out[s] = A.thr[path];
-                A.qacc_out[s] = A.acc[path];
-                A.qmisc_out[s] = make_uint4(__float_as_uint(A.brdf[path]), A.seed[path], A.flags[path], 0u);
+                A.ray_o_out[s] = A.def_o[i];
+                A.ray_d_out[s] = A.def_d[i];
+                A.qthr_out[s] = A.thr[i];
+                A.qacc_out[s] = A.def_a[i];
+                A.qmisc_out[s] = make_uint4(__float_as_uint(A.brdf[i]), A.seed[i], A.flags[i], 0u);
             }
         }
         return;
@@ -1273,25 +1281,24 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
         const uint32_t ia = pair * 2u * net::TILE + threadIdx.x, ib = ia + net::TILE;
         const bool va = ia < n, vb = ib < n;
         const uint32_t pa = va ? A.dq[ia] : 0u, pb = vb ? A.dq[ib] : 0u;
-        auto query = [&](bool v, uint32_t path, uint8_t* X) {
+        // origin and direction are stored by slot (rows ia and ib are read in order), the normal by path
+        auto query = [&](bool v, uint32_t slot, uint32_t path, uint8_t* X) {
             net::Query q{mk(0.0f, 0.0f, 0.0f), mk(0.0f, 1.0f, 0.0f), mk(0.0f, 1.0f, 0.0f)};
             if (v) {
-                const float4 o4 = A.def_o[path], d4 = A.def_d[path], dn = A.def_n[path];
+                const float4 o4 = A.def_o[slot], d4 = A.def_d[slot], dn = A.def_n[path];
                 q.pos = mk(o4.x, o4.y, o4.z);
                 q.n = mk(dn.x, dn.y, dn.z);
                 q.wo = mk(-d4.x, -d4.y, -d4.z);
-                // the sampling epilogue reads these after the network: start them toward L2 now
+                // the sampling epilogue reads these by path after the network: start them toward L2 now
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(A.def_t + path));
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(A.def_c + path));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.thr + path));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.acc + path));
             }
             float f[net::WIDTH];
             net::encode_features(q, A.box, f);
             net::store_row(X, net::X_RG, threadIdx.x, f);
         };
-        query(va, pa, XA);
-        query(vb, pb, XB);
+        query(va, ia, pa, XA);
+        query(vb, ib, pb, XB);
         bool ok = true;
         for (uint32_t l = 0; l < (uint32_t)net::LAYERS; ++l) {
             net::fence_async_smem();
@@ -1319,14 +1326,14 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
         if (!ok) break;
         for (uint32_t h = 0; h < 2u; ++h) {
             const bool v = h == 0u ? va : vb;
-            const uint32_t path = h == 0u ? pa : pb;
+            const uint32_t path = h == 0u ? pa : pb, q = h == 0u ? ia : ib;
             float raw[net::OUT];
             net::head_read(t_row + 64u * h, raw);
             bool go = false;
             if (v) {
                 net::Lobes L;
                 net::lobes_from_raw(raw, L);
-                guide_finish<Q, true, MARKOV>(A, path, &L, go);
+                guide_finish<Q, true, MARKOV>(A, q, path, &L, go);
             }
             const uint32_t mask = __ballot_sync(0xFFFFFFFFu, go);
             uint32_t slot = 0;
@@ -1335,11 +1342,11 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
             if (go) {
                 const uint32_t s = slot + __popc(mask & ((1u << lane) - 1u));
                 A.q_out[s] = path;
-                A.ray_o_out[s] = A.def_o[path];
-                A.ray_d_out[s] = A.def_d[path];
-                A.qthr_out[s] = A.thr[path];
-                A.qacc_out[s] = A.acc[path];
-                A.qmisc_out[s] = make_uint4(__float_as_uint(A.brdf[path]), A.seed[path], A.flags[path], 0u);
+                A.ray_o_out[s] = A.def_o[q];
+                A.ray_d_out[s] = A.def_d[q];
+                A.qthr_out[s] = A.thr[q];
+                A.qacc_out[s] = A.def_a[q];
+                A.qmisc_out[s] = make_uint4(__float_as_uint(A.brdf[q]), A.seed[q], A.flags[q], 0u);
             }
         }
     }
@@ -1519,6 +1526,7 @@ static int alloc_wave(WaveBuffers* w, uint32_t npix, bool full, bool guide, bool
         rc |= walloc(w, &w->def_c, P);
         rc |= walloc(w, &w->def_o, P);
         rc |= walloc(w, &w->def_d, P);
+        rc |= walloc(w, &w->def_a, P);
         rc |= walloc(w, &w->rec_head, P);
         rc |= walloc(w, &w->def_r, P);
         rc |= walloc(w, &w->def_kind, P);
@@ -2027,6 +2035,7 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         A.def_c = w->def_c;
         A.def_o = w->def_o;
         A.def_d = w->def_d;
+        A.def_a = w->def_a;
         A.def_r = w->def_r;
         A.def_kind = w->def_kind;
         A.def_lobe = w->def_lobe;

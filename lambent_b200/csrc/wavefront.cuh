@@ -45,8 +45,9 @@ struct Args {
     float4 *ray_o, *ray_d;          // rays by position in q_in (the generate kernel's queue is the identity)
     float4 *ray_o_out, *ray_d_out;  // rays by position in q_out, written where a path is appended
     // a live path's core state by position in q_in / q_out: throughput (xyz) and picked IOR (w); radiance
-    // sum (xyz) and cached pdf (w); (cached brdf bits, seed, flags, 0).  thr / acc / brdf / seed / flags
-    // below hold the same fields by path for deferred paths, and acc the radiance of finished paths.
+    // sum (xyz) and cached pdf (w); (cached brdf bits, seed, flags, 0).  thr / brdf / seed / flags below
+    // hold the same fields of a deferred vertex by its guide-queue slot, and acc the radiance of a
+    // finished path by path.
     float4 *qthr, *qacc;
     uint4* qmisc;
     float4 *qthr_out, *qacc_out;
@@ -81,10 +82,12 @@ struct Args {
     // outputs
     float4 *out_color, *out_normal, *out_albedo;
     v3 camera_pos;
-    // learned guiding
+    // learned guiding: the guide kernel's queue dq (path ids); a deferred vertex's normal and
+    // roughness, tangent and seed, albedo by path; its origin, incoming then outgoing direction, and
+    // sample colour and cached pdf by slot in dq (thr, brdf, seed and flags above hold the rest)
     uint32_t *dq, *dq_count;
     float4 *def_n, *def_t, *def_c;
-    float4 *def_o, *def_d;  // a deferred path's origin and incoming, then outgoing, direction (by path)
+    float4 *def_o, *def_d, *def_a;
     // learned + Markov guiding (three-way mixture): the Markov sampler's direction and pdf, and its
     // candidate lobes (mean, kappa) with their mixture weights (times the vMF branch's probability)
     float4* def_r;           // also a rough-metal vertex's reflection (xyz) and roughness y (w)
