@@ -621,6 +621,11 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
     G.mod_m = A.world_mod_m;
     G.camera_loc = A.camera_pos;
     const bool rec = A.ort != nullptr;
+    // learned guiding without Markov chains: what the bounce decides for a deferred vertex (normal and
+    // roughness, tangent and seed, albedo or the metal's reflection), held per thread until the append
+    // at the end gives the vertex its slot in the guide kernel's queue, where it is then written
+    constexpr bool STASH = LEARN && !GUIDE;
+    __shared__ float4 def_stash[STASH ? 3 : 1][STASH ? WAVE_BLOCK : 1];
     for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;; base += gridDim.x * blockDim.x) {
         if (base >= n) break;
         const uint32_t j = base + lane;  // work item; i: the queue position it shades
@@ -640,6 +645,7 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
             }
         }
         bool cont = false, deferred = false;
+        uint32_t def_kind = DEF_DIFFUSE;  // with `deferred`: what kind of vertex the guide kernel gets
         uint32_t path = 0;
         v3 ro = splat(0.0f), rd = splat(0.0f);  // the outgoing ray once the bounce is shaded
         float seg_w = 0.0f;                     // a batched path's segment, carried in the ray's w
@@ -862,10 +868,10 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                     if (LEARN && !GUIDE && is.ty == TY_DIFFUSE && depth + 1u < A.max_depth) {
                         // the guide kernel draws the direction; it uses the seeds of the cosine branch
                         deferred = true;
-                        A.def_kind[path] = DEF_DIFFUSE;
-                        A.def_n[path] = make_float4(is.normal.x, is.normal.y, is.normal.z, is.roughness.x);
-                        A.def_t[path] = make_float4(is.tangent.x, is.tangent.y, is.tangent.z, __uint_as_float(seed));
-                        A.def_c[path] = make_float4(is.color.x, is.color.y, is.color.z, 0.0f);
+                        def_kind = DEF_DIFFUSE;
+                        def_stash[0][threadIdx.x] = make_float4(is.normal.x, is.normal.y, is.normal.z, is.roughness.x);
+                        def_stash[1][threadIdx.x] = make_float4(is.tangent.x, is.tangent.y, is.tangent.z, __uint_as_float(seed));
+                        def_stash[2][threadIdx.x] = make_float4(is.color.x, is.color.y, is.color.z, 0.0f);
                         seed += 3u;
                     } else if (is.ty == TY_DIFFUSE) {
                         v3 dir_cos = cosine_hemisphere(seed, is.normal, is.tangent);
@@ -968,10 +974,20 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                         // the guide kernel mixes this reflection with the network's lobes (the path's
                         // throughput already holds the albedo, the whole weight of this bounce)
                         deferred = true;
-                        A.def_kind[path] = DEF_METAL;
-                        A.def_n[path] = make_float4(is.normal.x, is.normal.y, is.normal.z, is.roughness.x);
-                        A.def_t[path] = make_float4(is.tangent.x, is.tangent.y, is.tangent.z, __uint_as_float(seed));
-                        A.def_r[path] = make_float4(rd.x, rd.y, rd.z, is.roughness.y);
+                        def_kind = DEF_METAL;
+                        const float4 dn = make_float4(is.normal.x, is.normal.y, is.normal.z, is.roughness.x);
+                        const float4 dt = make_float4(is.tangent.x, is.tangent.y, is.tangent.z, __uint_as_float(seed));
+                        const float4 dr = make_float4(rd.x, rd.y, rd.z, is.roughness.y);
+                        if (STASH) {
+                            def_stash[0][threadIdx.x] = dn;
+                            def_stash[1][threadIdx.x] = dt;
+                            def_stash[2][threadIdx.x] = dr;
+                        } else {
+                            A.def_kind[path] = DEF_METAL;
+                            A.def_n[path] = dn;
+                            A.def_t[path] = dt;
+                            A.def_r[path] = dr;
+                        }
                         rd = rd_in;  // the deferred path keeps its incoming direction
                     }
                 }
@@ -1036,6 +1052,13 @@ __global__ void __launch_bounds__(WAVE_BLOCK, (GUIDE ? 1 : 6)) shade_kernel(cons
                     A.brdf[q] = __uint_as_float(o_misc.x);
                     A.seed[q] = o_misc.y;
                     A.flags[q] = o_misc.z;
+                    if (STASH) {
+                        A.def_kind[q] = def_kind;
+                        A.def_n[q] = def_stash[0][threadIdx.x];
+                        A.def_t[q] = def_stash[1][threadIdx.x];
+                        if (def_kind == DEF_METAL) A.def_r[q] = def_stash[2][threadIdx.x];
+                        else A.def_c[q] = def_stash[2][threadIdx.x];
+                    }
                 }
             }
         }
@@ -1113,7 +1136,8 @@ LAM_DEV void record_vertex(const Args& A, uint32_t path, uint32_t seed0, v3 ro, 
 // bounce, unchanged.
 template <bool NET, bool MARKOV>
 LAM_DEV void guide_finish_metal(const Args& A, uint32_t q, uint32_t path, const net::Lobes* L) {
-    const float4 d4 = A.def_d[q], dn = A.def_n[path], dt = A.def_t[path], dr = A.def_r[path];
+    const uint32_t v = MARKOV ? path : q;  // where the shade kernel left the vertex's records
+    const float4 d4 = A.def_d[q], dn = A.def_n[v], dt = A.def_t[v], dr = A.def_r[v];
     v3 dir = mk(dr.x, dr.y, dr.z);
     if (NET) {
         const float4 th = A.thr[q];
@@ -1143,16 +1167,19 @@ LAM_DEV void guide_finish_metal(const Args& A, uint32_t q, uint32_t path, const 
 }
 
 // The vertex at guide queue slot q of path `path`: its live state (origin, direction, throughput,
-// sample colour, brdf, seed, flags) is stored by slot, what the shade kernel decided at the vertex
-// (kind, frame, albedo, the Markov draw and lobes) by path, as are its training records.
+// sample colour, brdf, seed, flags) is stored by slot.  What the shade kernel decided at the vertex
+// (kind, frame, albedo, the metal's reflection) is stored by slot too, except after the Markov-guided
+// shade kernel (MARKOV), which keeps it and the Markov draw and lobes by path.  Training records are
+// kept by path.
 template <int Q, bool NET, bool MARKOV>
 LAM_DEV void guide_finish(const Args& A, uint32_t q, uint32_t path, const net::Lobes* L, bool& out) {
-    if (A.def_kind[path] == DEF_METAL) {
+    const uint32_t v = MARKOV ? path : q;
+    if (A.def_kind[v] == DEF_METAL) {
         guide_finish_metal<NET, MARKOV>(A, q, path, L);
         out = true;
         return;
     }
-    const float4 o4 = A.def_o[q], d4 = A.def_d[q], dn = A.def_n[path], dt = A.def_t[path], dc = A.def_c[path];
+    const float4 o4 = A.def_o[q], d4 = A.def_d[q], dn = A.def_n[v], dt = A.def_t[v], dc = A.def_c[v];
     const float4 th = A.thr[q], ac = A.def_a[q];
     const v3 ro = mk(o4.x, o4.y, o4.z), rd = mk(d4.x, d4.y, d4.z), n = mk(dn.x, dn.y, dn.z), t = mk(dt.x, dt.y, dt.z);
     const uint32_t seed0 = __float_as_uint(dt.w);
@@ -1281,17 +1308,19 @@ __global__ void __launch_bounds__(WAVE_BLOCK) guide_sample_kernel(Args A) {
         const uint32_t ia = pair * 2u * net::TILE + threadIdx.x, ib = ia + net::TILE;
         const bool va = ia < n, vb = ib < n;
         const uint32_t pa = va ? A.dq[ia] : 0u, pb = vb ? A.dq[ib] : 0u;
-        // origin and direction are stored by slot (rows ia and ib are read in order), the normal by path
+        // origin and direction are stored by slot (rows ia and ib are read in order); the normal too,
+        // except after the Markov-guided shade kernel, which keeps it by path
         auto query = [&](bool v, uint32_t slot, uint32_t path, uint8_t* X) {
             net::Query q{mk(0.0f, 0.0f, 0.0f), mk(0.0f, 1.0f, 0.0f), mk(0.0f, 1.0f, 0.0f)};
             if (v) {
-                const float4 o4 = A.def_o[slot], d4 = A.def_d[slot], dn = A.def_n[path];
+                const uint32_t r = MARKOV ? path : slot;
+                const float4 o4 = A.def_o[slot], d4 = A.def_d[slot], dn = A.def_n[r];
                 q.pos = mk(o4.x, o4.y, o4.z);
                 q.n = mk(dn.x, dn.y, dn.z);
                 q.wo = mk(-d4.x, -d4.y, -d4.z);
-                // the sampling epilogue reads these by path after the network: start them toward L2 now
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.def_t + path));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.def_c + path));
+                // the sampling epilogue reads these after the network: start them toward L2 now
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.def_t + r));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(A.def_c + r));
             }
             float f[net::WIDTH];
             net::encode_features(q, A.box, f);

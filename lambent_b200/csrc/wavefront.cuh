@@ -83,8 +83,9 @@ struct Args {
     float4 *out_color, *out_normal, *out_albedo;
     v3 camera_pos;
     // learned guiding: the guide kernel's queue dq (path ids); a deferred vertex's normal and
-    // roughness, tangent and seed, albedo by path; its origin, incoming then outgoing direction, and
-    // sample colour and cached pdf by slot in dq (thr, brdf, seed and flags above hold the rest)
+    // roughness, tangent and seed, albedo (by slot in dq, by path after the Markov-guided shade
+    // kernel); its origin, incoming then outgoing direction, and sample colour and cached pdf by slot
+    // in dq (thr, brdf, seed and flags above hold the rest)
     uint32_t *dq, *dq_count;
     float4 *def_n, *def_t, *def_c;
     float4 *def_o, *def_d, *def_a;
