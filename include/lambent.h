@@ -490,11 +490,11 @@ int lam_pipeline_set_wave_paths(lam_pipeline* pipeline, uint64_t max_paths);
  * thread).  LAM_SHADE_ORDER_QUEUE shades the queued hits in the order extend found them;
  * LAM_SHADE_ORDER_MATERIAL first sorts them (stable) by what the bounce runs: sky, diffuse,
  * metallic, transparent, so that a warp's lanes take the same branch.  LAM_SHADE_ORDER_AUTO, the
- * default, sorts unguided renders only: Markov-guided and learned-guide renders run slower in class
- * order.  A plain render's image does not depend on the order;
+ * default, sorts every render except Markov-guided ones, which run slower in class order.  A plain
+ * render's image does not depend on the order;
  * under guiding, the world-grid and training updates land in another order, as they already may
  * between two runs.  The sort keeps 5 bytes per path of device state.  Takes effect at the next
- * lam_render or lam_batch_render (which runs no guiding, so that AUTO sorts there). */
+ * lam_render or lam_batch_render. */
 #define LAM_SHADE_ORDER_AUTO 0u
 #define LAM_SHADE_ORDER_QUEUE 1u
 #define LAM_SHADE_ORDER_MATERIAL 2u

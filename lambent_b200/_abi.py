@@ -33,7 +33,7 @@ RESTIR_DISABLED, RESTIR_PER_SAMPLE, RESTIR_PER_PIXEL = 0, 1, 2
 GUIDE_NONE, GUIDE_MARKOV, GUIDE_LEARNED = 0, 1, 2
 GUIDE_PDF_AT_SAMPLE = 4  # modifier of GUIDE_MARKOV: mixture pdf with its cosine term at the chosen direction
 GUIDE_METAL = 8  # modifier of the learned modes: mix the learned lobes in at rough metallic vertices too
-SHADE_ORDER_AUTO = 0      # lam_pipeline_set_shade_order: material order for unguided renders
+SHADE_ORDER_AUTO = 0      # lam_pipeline_set_shade_order: material order except under Markov guiding
 SHADE_ORDER_QUEUE = 1     # traversal order
 SHADE_ORDER_MATERIAL = 2  # sorted by shading class (sky, diffuse, metallic, transparent)
 BUFFER_MARKOV_CHAIN_SCREEN_SPACE, BUFFER_SPATIAL_RESAMPLING, BUFFER_MARKOV_CHAIN_WORLD_SPACE = 1, 2, 4

@@ -437,7 +437,7 @@ class Pipeline:
     def set_shade_order(self, order=_abi.SHADE_ORDER_AUTO):
         """SHADE_ORDER_MATERIAL sorts each bounce's hits by class (sky, diffuse, metallic,
         transparent) before shading; SHADE_ORDER_QUEUE shades them in traversal order;
-        SHADE_ORDER_AUTO (the default) sorts unguided renders only."""
+        SHADE_ORDER_AUTO (the default) sorts except under Markov guiding."""
         check(lib().lam_pipeline_set_shade_order(self._h, int(order)))
 
     def profile(self):

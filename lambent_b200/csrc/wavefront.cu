@@ -2075,9 +2075,8 @@ extern "C" int lam_render(lam_pipeline* pl, const lam_scene* s, lam_data_buffers
         std::memcpy(A.box, s->bounds, sizeof(A.box));
     }
     if (guide && !world) return set_error(LAM_ERR_INVALID_ARGUMENT, "Markov guiding needs MARKOV_CHAIN_WORLD_SPACE buffers");
-    // automatic order: sorted for unguided renders; both guided forms measured faster in queue order
-    const bool sorted = pl->shade_order == LAM_SHADE_ORDER_MATERIAL ||
-                        (pl->shade_order == LAM_SHADE_ORDER_AUTO && !guide && !learned);
+    // automatic order: sorted except under Markov guiding, which measured faster in queue order
+    const bool sorted = pl->shade_order == LAM_SHADE_ORDER_MATERIAL || (pl->shade_order == LAM_SHADE_ORDER_AUTO && !guide);
     if (sorted) {
         if (!w->shade_order && (walloc(w, &w->shade_key, w->paths) || walloc(w, &w->shade_order, w->paths) ||
                                 walloc(w, &w->shade_bc, (size_t)SORT_BLOCKS_MAX * SHADE_CLASSES)))
