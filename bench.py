@@ -30,19 +30,20 @@ SEG_BYTES_EXTEND = 48   # ray (o, d, tmax) 28 B read + hit 20 B write per segmen
 SEG_BYTES_TOTAL = 280   # extend 48 + shade 232 (compulsory wavefront traffic per segment)
 # DRAM bytes (read + write) per segment of the extend kernel: ncu's dram__bytes_read.sum +
 # dram__bytes_write.sum over the 12 extend launches of one 960x540, 4-spp step of the same scene
-# (7.20M segments; the full 1080p step is too large for a multi-metric capture), from
+# (7.20M segments; the full 1080p step is too large for a multi-metric capture), in the default
+# material-ordered shading, from
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum,lts__t_sector_hit_rate.pct
 #       --clock-control none -k regex:extend_kernel -s 36 -c 12 python bench.py --width 960 --height 540 --spp 4
 #       --steps 1 --warmup 3 --no-cpu-baseline --no-guided --no-batched --no-restir
 # Traffic grows with the segments a launch processes, so a full launch's traffic is this times its segments.
-EXTEND_DRAM_BYTES_PER_SEGMENT = 134.5
+EXTEND_DRAM_BYTES_PER_SEGMENT = 132.4
 # What does bound the traversal kernel, from an ncu capture of two extend launches of the same
 # 960x540 case (sections SpeedOfLight, ComputeWorkloadAnalysis, MemoryWorkloadAnalysis,
 # WarpStateStats; command beside the figures in the extend-kernel profile summary): instruction issue.
-EXTEND_MEASURED_BOUND = {"kind": "instruction issue (BVH and triangles stay in L2)", "issue_slots_busy": 0.741,
-                         "alu_pipe": 0.587, "fma_pipe": 0.257, "dram_throughput": 0.010, "l2_throughput": 0.114,
-                         "l2_hit_rate": 0.802, "threads_per_instruction": 18.9, "warps_active": 0.363,
-                         "stalls_per_issue": {"wait": 1.90, "not_selected": 1.45, "long_scoreboard": 1.11},
+EXTEND_MEASURED_BOUND = {"kind": "instruction issue (BVH and triangles stay in L2)", "issue_slots_busy": 0.750,
+                         "alu_pipe": 0.588, "fma_pipe": 0.254, "dram_throughput": 0.010, "l2_throughput": 0.109,
+                         "l2_hit_rate": 0.797, "threads_per_instruction": 18.9, "warps_active": 0.363,
+                         "stalls_per_issue": {"wait": 1.95, "not_selected": 1.38, "long_scoreboard": 1.22},
                          "note": "mean of two launches of the 960x540, 4-spp case"}
 
 
