@@ -483,12 +483,14 @@ LAM_DEV void finalize_records(const Args& A, uint32_t path, v3 scol) {
 }
 
 // ---------------------------------------------------------------- material-ordered shading
-// A stable counting sort of the queue by shading class.  A warp that holds sky, diffuse, metallic
-// and transparent lanes runs each class's code in turn with the other lanes idle; in class order
-// the warps are uniform but for the last one of each class.  The three kernels split the queue
-// into one contiguous chunk per block: count the classes of the chunk, scan the counts (class
-// major, then block), and write each position to its slot in the order.  Within a class the queue
-// order is kept, so the shade kernel's reads stay nearly sequential.
+// A stable counting sort of the queue by shading class (sky, diffuse, metallic, transparent), so that
+// the shade kernel runs one class at a time across the whole GPU: its warps take one branch, and
+// every SM's caches hold one class's code, materials and textures.  (A sort within blocks, whose
+// warps are as uniform, gave no gain: the grid-wide order is what pays.)  The three kernels split
+// the queue into one contiguous chunk per block: count the classes of the chunk, scan the counts
+// (class major, then block), and write each position to its slot in the order.  Within a class the
+// queue order is kept, so the shade kernel's reads stay nearly sequential.  A procedural hit's
+// leaf record holds its primitive in the same word as a triangle's.
 
 LAM_DEV uint32_t shade_class(const DevScene& S, uint2 h) {
     if (h.x == NO_HIT) return SHADE_SKY;
