@@ -470,6 +470,29 @@ impl Pipeline {
         check(unsafe { sys::lam_render_stats_get(self.h, &mut s) })?;
         Ok(s)
     }
+
+    /// Bounds the paths of one wave (about 220 bytes of device state each); 0 restores the default of
+    /// about 32M paths.  The image does not depend on it.  No counterpart in the reference.
+    pub fn set_wave_paths(&mut self, max_paths: u64) -> Result<(), Error> {
+        check(unsafe { sys::lam_pipeline_set_wave_paths(self.h, max_paths) })
+    }
+
+    /// The order in which each bounce's hits are shaded.  No counterpart in the reference.
+    pub fn set_shade_order(&mut self, order: ShadeOrder) -> Result<(), Error> {
+        check(unsafe { sys::lam_pipeline_set_shade_order(self.h, order as u32) })
+    }
+}
+
+/// Shading order of a pipeline's bounces: `Material` sorts each bounce's hits by shading class (sky,
+/// diffuse, metallic, transparent) before shading, `Queue` shades them in traversal order, and
+/// `Auto`, the default, sorts except under Markov guiding.  A plain render's image is the same in
+/// every order.
+#[repr(u32)]
+#[derive(Clone, Copy, Debug, PartialEq, Eq)]
+pub enum ShadeOrder {
+    Auto = sys::LAM_SHADE_ORDER_AUTO,
+    Queue = sys::LAM_SHADE_ORDER_QUEUE,
+    Material = sys::LAM_SHADE_ORDER_MATERIAL,
 }
 
 impl Drop for Pipeline {
