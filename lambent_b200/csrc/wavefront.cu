@@ -492,13 +492,6 @@ LAM_DEV void finalize_records(const Args& A, uint32_t path, v3 scol) {
 // queue order is kept, so the shade kernel's reads stay nearly sequential.  A procedural hit's
 // leaf record holds its primitive in the same word as a triangle's.
 
-LAM_DEV uint32_t shade_class(const DevScene& S, uint2 h) {
-    if (h.x == NO_HIT) return SHADE_SKY;
-    const uint32_t prim = __float_as_uint(ld_keep(S.tris + 3u * h.x).w);
-    const uint32_t ty = load_material(S, h.y, prim).tex_idx_attributes_ty >> 16;
-    return ty == TY_METALLIC ? SHADE_METALLIC : (ty == TY_TRANSPARENT ? SHADE_TRANSPARENT : SHADE_DIFFUSE);
-}
-
 // The chunk of queue positions [*beg, *end) of block b of nb (a multiple of the block size).
 LAM_DEV void sort_chunk(uint32_t n, uint32_t b, uint32_t nb, uint32_t* beg, uint32_t* end) {
     const uint32_t per = (n + nb - 1u) / nb;
@@ -516,21 +509,58 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_keys_kernel(const __grid_con
     uint32_t beg, end;
     sort_chunk(*A.count_in, blockIdx.x, gridDim.x, &beg, &end);
     const uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t t = beg; t < end; t += WAVE_BLOCK) {
-        const uint32_t j = t + threadIdx.x;
-        uint32_t k = SHADE_CLASSES;
-        if (j < end) {
+    // U tiles per step, each stage's loads issued for all of them before the next stage's: a class
+    // is a chain of four dependent loads (hit; triangle word and instance; material index; material)
+    constexpr uint32_t U = 4;
+    for (uint32_t t = beg; t < end; t += U * WAVE_BLOCK) {
+        bool v[U];
+        uint2 h[U];
+        const DevScene* S[U];
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) {
+            const uint32_t j = t + q * WAVE_BLOCK + threadIdx.x;
+            v[q] = j < end;
+            S[q] = &A.S;
             // plain loads: the shade kernel reads the hit (and a batched path's flags) again next
-            const DevScene* S = &A.S;
-            if (BATCH) S = &A.reqs[A.segs[A.qmisc[j].z >> 16].req].S;
-            k = shade_class(*S, A.hit[j]);
-            A.shade_key[j] = (uint8_t)k;
+            if (BATCH && v[q]) S[q] = &A.reqs[A.segs[A.qmisc[j].z >> 16].req].S;
+            h[q] = v[q] ? A.hit[j] : make_uint2(NO_HIT, 0u);
+        }
+        uint32_t prim[U], mcount[U], moff[U];
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) {
+            const bool hit = h[q].x != NO_HIT;
+            prim[q] = hit ? __float_as_uint(ld_keep(S[q]->tris + 3u * h[q].x).w) : 0u;
+            mcount[q] = hit ? S[q]->inst[h[q].y].mat_count : 0u;
+            moff[q] = hit ? S[q]->inst[h[q].y].mat_offset : 0u;
+        }
+        uint32_t mi[U];
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q)
+            mi[q] = clamp_idx(mcount[q] ? __ldg(S[q]->mat_idx + moff[q] + clamp_idx(prim[q], mcount[q])) : 0u,
+                              S[q]->material_count);
+        uint32_t k[U];
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) {
+            const uint32_t j = t + q * WAVE_BLOCK + threadIdx.x;
+            k[q] = SHADE_CLASSES;
+            if (v[q]) {
+                if (h[q].x == NO_HIT) {
+                    k[q] = SHADE_SKY;
+                } else {
+                    // tex_idx_attributes_ty: the type in its upper half (as load_material reads it)
+                    const uint32_t ty = __ldg(reinterpret_cast<const uint32_t*>(S[q]->materials + mi[q]) + 5) >> 16;
+                    k[q] = ty == TY_METALLIC ? SHADE_METALLIC : (ty == TY_TRANSPARENT ? SHADE_TRANSPARENT : SHADE_DIFFUSE);
+                }
+                A.shade_key[j] = (uint8_t)k[q];
+            }
         }
 #pragma unroll
-        for (uint32_t c = 0; c < SHADE_CLASSES; ++c) {
-            const uint32_t m = __ballot_sync(0xFFFFFFFFu, k == c);
-            if (lane == 0u && m) atomicAdd(&cnt[c], (uint32_t)__popc(m));
-        }
+        for (uint32_t q = 0; q < U; ++q)
+#pragma unroll
+            for (uint32_t c = 0; c < SHADE_CLASSES; ++c) {
+                const uint32_t m = __ballot_sync(0xFFFFFFFFu, k[q] == c);
+                if (lane == 0u && m) atomicAdd(&cnt[c], (uint32_t)__popc(m));
+            }
     }
     __syncthreads();
     if (threadIdx.x < SHADE_CLASSES) A.shade_bc[blockIdx.x * SHADE_CLASSES + threadIdx.x] = cnt[threadIdx.x];
