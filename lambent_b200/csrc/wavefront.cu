@@ -602,8 +602,10 @@ __global__ void __launch_bounds__(SORT_BLOCKS_MAX) shade_scan_kernel(const __gri
 }
 
 __global__ void __launch_bounds__(WAVE_BLOCK) shade_scatter_kernel(const __grid_constant__ Args A) {
-    constexpr uint32_t NW = WAVE_BLOCK / 32;
-    __shared__ uint32_t wcnt[NW][SHADE_CLASSES];
+    // U tiles per step: their ranks come from one pass of ballots, so that a step takes three
+    // barriers instead of three per tile
+    constexpr uint32_t NW = WAVE_BLOCK / 32, U = 4;
+    __shared__ uint32_t wcnt[U][NW][SHADE_CLASSES];
     __shared__ uint32_t next[SHADE_CLASSES];
     if (threadIdx.x < SHADE_CLASSES) next[threadIdx.x] = A.shade_bc[blockIdx.x * SHADE_CLASSES + threadIdx.x];
     __syncthreads();
@@ -611,27 +613,40 @@ __global__ void __launch_bounds__(WAVE_BLOCK) shade_scatter_kernel(const __grid_
     sort_chunk(*A.count_in, blockIdx.x, gridDim.x, &beg, &end);
     const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
     const uint32_t below = (1u << lane) - 1u;
-    for (uint32_t t = beg; t < end; t += WAVE_BLOCK) {
-        const uint32_t j = t + threadIdx.x;
-        const uint32_t k = j < end ? (uint32_t)A.shade_key[j] : SHADE_CLASSES;
-        uint32_t rank = 0u;
+    for (uint32_t t = beg; t < end; t += U * WAVE_BLOCK) {
+        uint32_t k[U], rank[U];
 #pragma unroll
-        for (uint32_t c = 0; c < SHADE_CLASSES; ++c) {
-            const uint32_t m = __ballot_sync(0xFFFFFFFFu, k == c);
-            if (k == c) rank = (uint32_t)__popc(m & below);
-            if (lane == 0u) wcnt[wid][c] = (uint32_t)__popc(m);
+        for (uint32_t q = 0; q < U; ++q) {
+            const uint32_t j = t + q * WAVE_BLOCK + threadIdx.x;
+            k[q] = j < end ? (uint32_t)A.shade_key[j] : SHADE_CLASSES;
+            rank[q] = 0u;
+#pragma unroll
+            for (uint32_t c = 0; c < SHADE_CLASSES; ++c) {
+                const uint32_t m = __ballot_sync(0xFFFFFFFFu, k[q] == c);
+                if (k[q] == c) rank[q] = (uint32_t)__popc(m & below);
+                if (lane == 0u) wcnt[q][wid][c] = (uint32_t)__popc(m);
+            }
         }
         __syncthreads();
-        if (k < SHADE_CLASSES) {
-            uint32_t slot = next[k] + rank;
-            for (uint32_t w = 0; w < wid; ++w) slot += wcnt[w][k];
-            A.shade_order[slot] = j;
+        // a position's slot: its class's next slot, then the earlier tiles' and earlier warps' lanes
+        // of its class, then its rank within its warp (stable: tiles, warps and lanes in order)
+#pragma unroll
+        for (uint32_t q = 0; q < U; ++q) {
+            if (k[q] < SHADE_CLASSES) {
+                uint32_t slot = next[k[q]] + rank[q];
+                for (uint32_t p = 0; p < q; ++p)
+                    for (uint32_t w = 0; w < NW; ++w) slot += wcnt[p][w][k[q]];
+                for (uint32_t w = 0; w < wid; ++w) slot += wcnt[q][w][k[q]];
+                A.shade_order[slot] = t + q * WAVE_BLOCK + threadIdx.x;
+            }
         }
         __syncthreads();
         if (threadIdx.x < SHADE_CLASSES) {
             uint32_t add = 0u;
 #pragma unroll
-            for (uint32_t w = 0; w < NW; ++w) add += wcnt[w][threadIdx.x];
+            for (uint32_t q = 0; q < U; ++q)
+#pragma unroll
+                for (uint32_t w = 0; w < NW; ++w) add += wcnt[q][w][threadIdx.x];
             next[threadIdx.x] += add;
         }
         __syncthreads();
