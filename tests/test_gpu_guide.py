@@ -238,16 +238,18 @@ def test_learned_and_markov_three_way_mixture_is_unbiased(cuda):
     """LEARNED | MARKOV: the network's lobes, the cosine lobe and the Markov chains' vMF lobes in one
     one-sample-MIS mixture (the Markov sampler's draw with probability 1 - f, the network's with f,
     weighted by (1 - f) p_markov + f q).  Trained on its first 32 spp, it agrees with plain path
-    tracing on 16 x 16 blocks within 4.5 sigma, and beats plain path tracing in relMSE at equal spp.
-    A render's relMSE here is heavy-tailed (a few bright pixels from the racing Markov chains carry
-    most of it), so the median over the renders is compared."""
+    tracing on 16 x 16 blocks within 5 sigma, and beats plain path tracing in relMSE at equal spp.
+    The estimator is heavy-tailed (a few bright pixels from the racing Markov chains): the block
+    test takes 16 renders of each and allows 5 sigma over its 48 block-channel comparisons (with
+    8 renders and 4.5 sigma a correct build failed it once in five runs, at 4.53), and the gain
+    test compares the median relMSE over the renders."""
     s = scenes.occluded_cornell(64, 64)
     mode = _abi.GUIDE_LEARNED | _abi.GUIDE_MARKOV
     g = _guide(train_spp=32, record_capacity=1 << 18, batch=8192, steps_per_wave=8, seed=5)
     _, gpipe, gs = _render_markov(s, 32, mode, g, seed=1000)
     steps, spp = g.progress()
     assert steps == 32 * 8 and spp == 32
-    reps, spp = 8, 64
+    reps, spp = 16, 64
     three = [_render_markov(s, spp, mode, seed=2000 + k, pipe=gpipe, gscene=gs)[0] for k in range(reps)]
     assert g.progress()[0] == 32 * 8
     ppipe = None
@@ -260,7 +262,7 @@ def test_learned_and_markov_three_way_mixture_is_unbiased(cuda):
     pb = np.stack([_block_means(x) for x in plain])
     se = np.sqrt(tb.var(axis=0, ddof=1) / reps + pb.var(axis=0, ddof=1) / reps) + 1e-6
     z = np.abs(tb.mean(axis=0) - pb.mean(axis=0)) / se
-    assert np.all(z < 4.5), z.max()
+    assert np.all(z < 5.0), z.max()
 
     def relmse(x):
         return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))
