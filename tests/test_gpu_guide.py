@@ -192,7 +192,7 @@ def test_trained_guide_is_unbiased_and_reduces_error(cuda):
     _, gpipe, gs = _render(s, 64, _abi.GUIDE_LEARNED, g, seed=1000)
     steps, spp = g.progress()
     assert steps == 200 and spp == 64
-    reps, spp = 16, 64  # 16 renders a side: the block test's standard errors from 8 were loose
+    reps, spp = 16, 64  # with 8 a side, the 48 block comparisons' standard errors are too loose for 4.5 sigma
     guided = [_render(s, spp, seed=2000 + k, pipe=gpipe, gscene=gs)[0] for k in range(reps)]
     assert g.progress()[0] == 200  # no further training
     ppipe = None
@@ -306,7 +306,7 @@ def test_guide_at_rough_metal_vertices_is_unbiased(cuda):
     assert np.array_equal(plain, untrained)
     g = _guide(train_spp=64, record_capacity=1 << 20, batch=8192, steps_per_wave=200, seed=9)
     _, gpipe, gs = _render(s, 64, mode, g, seed=1000)
-    reps, spp = 16, 64  # 16 renders a side: the block test's standard errors from 8 were loose
+    reps, spp = 16, 64  # with 8 a side, the 48 block comparisons' standard errors are too loose for 4.5 sigma
     guided = [_render(s, spp, seed=2000 + k, pipe=gpipe, gscene=gs)[0] for k in range(reps)]
     ppipe, plain = None, []
     for k in range(reps):
